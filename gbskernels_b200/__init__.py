@@ -1,0 +1,570 @@
+"""gbskernels_b200 -- B200-native (sm_100a) batched permanents, hafnians, loop
+hafnians and torontonians behind the ``gbskernels`` API of chaofanzhougit/GBSKernels.
+
+Drop-in for the reference's ``backend="gpu"`` path (gbskernels/__init__.py:517-908):
+the same function names, signatures, precision tiers, return shapes, diagnostics
+dictionaries and exception types.  Everything runs in ``libgbs_b200.so`` (C++ host
+runtime + hand-written sm_100a kernels) through its C ABI; this module only
+marshals numpy arrays.  There is no CPU backend here and no CPU fallback: the
+reference's CPU backend (``backend="cpu"``) and its mpmath tier (``"ref"``) stay
+in the reference package.
+
+Precision tiers (as in the reference):
+  * ``"fp64"``      binary64 throughout (power trace products on FP64 tensor cores);
+  * ``"dd"``        double-double value path;
+  * ``"auto"``      fp64 plus the cancellation indicator kappa = sum|term| / |value|,
+                    elements with kappa >= 1e8 rerun in double-double ON THE DEVICE
+                    (the reference's CPU mpmath rerun does not exist here);
+  * ``"certified"`` value plus a rigorous bound |value - exact| <= abs_error_bound.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Any, Iterable
+
+import numpy as np
+
+from . import _lib
+
+__version__ = "0.1.0"
+__all__ = [
+    "perm", "perm_batched", "haf", "haf_batched", "lhaf", "lhaf_batched",
+    "tor", "tor_batched", "tor_single", "gpu_available", "gpu_backend_kind",
+    "Workspace", "PRECISIONS", "queue_evaluate",
+]
+
+PRECISIONS = ("fp64", "ref", "dd", "auto", "certified")
+_FN = {"perm": 0, "haf": 1, "lhaf": 2, "tor": 3}
+_TIER = {"fp64": 0, "dd": 1, "kappa": 2}
+_AUTO_KAPPA_MAX = 1e8  # gbskernels/__init__.py:240
+
+# Largest input side each kernel family supports (tor: 2n).
+_GPU_MAX_DIM = {
+    "perm": 28, "perm_dd": 28,
+    "haf": 32, "haf_dd": 32,
+    "lhaf": 32, "lhaf_dd": 32,
+    "tor": 48, "tor_dd": 48,
+}
+
+
+# ------------------------------------------------------------------ helpers
+def _check_backend(backend: str) -> None:
+    if backend == "gpu":
+        return
+    if backend == "cpu":
+        raise NotImplementedError(
+            "gbskernels_b200 implements backend='gpu' only; the CPU backend is the "
+            "reference package's cpu_ref")
+    raise ValueError(f"unknown backend {backend!r}; expected 'cpu' or 'gpu'")
+
+
+def _as_stack(matrices: Iterable[Any]) -> np.ndarray:
+    stack = np.ascontiguousarray(np.asarray(matrices, dtype=np.complex128))
+    if stack.ndim != 3 or stack.shape[1] != stack.shape[2]:
+        raise ValueError(
+            "GPU backend needs a uniform (B, d, d) stack of square matrices; "
+            "ragged batches go through gbskernels_b200.Workspace.")
+    return stack
+
+
+def _prepare(func: str, matrices: Iterable[Any], precision: str) -> np.ndarray:
+    """Validate a uniform bucket (gbskernels/__init__.py:158-219 semantics)."""
+    if precision not in ("fp64", "dd"):
+        if precision == "ref":
+            raise NotImplementedError(
+                "'ref' is the mpmath ground truth -- CPU only (backend='cpu').")
+        raise ValueError(f"unknown precision {precision!r}; expected one of {PRECISIONS}")
+    stack = _as_stack(matrices)
+    d = int(stack.shape[1])
+    name = func if precision == "fp64" else f"{func}_dd"
+    deff = d + (d & 1) if func == "lhaf" else d
+    if func == "tor" and d % 2:
+        raise ValueError("torontonian requires an even dimension 2n")
+    if deff > _GPU_MAX_DIM[name]:
+        raise ValueError(f"GPU {name}: matrix dimension {d} exceeds the kernel's limit "
+                         f"{_GPU_MAX_DIM[name]}")
+    if func == "tor" and stack.size and float(np.max(np.abs(stack.imag))) > 0.0:
+        if precision == "dd":
+            raise ValueError("GPU torontonian (precision='dd') is real-domain only; the input "
+                             "has non-zero imaginary parts.")
+    return stack
+
+
+def _kernel_dim(func: str, d: int) -> int:
+    return d // 2 if func == "tor" else d
+
+
+def _call_uniform(func: str, stack: np.ndarray, precision: str) -> np.ndarray:
+    lib = _lib.load()
+    B, d = stack.shape[0], stack.shape[1]
+    out = np.empty(B, dtype=np.complex128)
+    if B == 0:
+        return out
+    name = f"gbs_{func}_host" if precision == "fp64" else f"gbs_{func}_dd_host"
+    fn = getattr(lib, name)
+    rc = fn(_lib.dptr(stack.view(np.float64)), _kernel_dim(func, d), B, _lib.dptr(out.view(np.float64)))
+    _lib.check(rc, name)
+    return out
+
+
+def _call_aux(func: str, stack: np.ndarray, kind: str) -> tuple[np.ndarray, np.ndarray]:
+    lib = _lib.load()
+    B, d = stack.shape[0], stack.shape[1]
+    out = np.empty(B, dtype=np.complex128)
+    aux = np.empty(B, dtype=np.float64)
+    if B == 0:
+        return out, aux
+    name = f"gbs_{func}_{kind}_host"
+    fn = getattr(lib, name, None)
+    if fn is None:
+        raise NotImplementedError(f"libgbs_b200 has no {name}")
+    rc = fn(_lib.dptr(stack.view(np.float64)), _kernel_dim(func, d), B, _lib.dptr(out.view(np.float64)),
+            _lib.dptr(aux))
+    _lib.check(rc, name)
+    return out, aux
+
+
+# ------------------------------------------------------------------ tiers
+def _auto_batched(func: str, matrices, return_diagnostics: bool):
+    stack = _prepare(func, matrices, "fp64")
+    lib = _lib.load()
+    B, d = stack.shape[0], stack.shape[1]
+    out = np.empty(B, dtype=np.complex128)
+    kappa = np.empty(B, dtype=np.float64)
+    tier = np.empty(B, dtype=np.int32)
+    if B:
+        rc = lib.gbs_auto_host(_FN[func], _lib.dptr(stack.view(np.float64)), d, B, _AUTO_KAPPA_MAX,
+                               _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier))
+        _lib.check(rc, "gbs_auto_host")
+    if not return_diagnostics:
+        return out
+    diags = [{"tier": "dd" if t else "fp64", "cancellation": float(k)} for t, k in zip(tier, kappa)]
+    return out, diags
+
+
+def _finite_certificate(value: complex, bound: float) -> bool:
+    return (np.isfinite(value.real) and np.isfinite(value.imag) and np.isfinite(bound) and bound >= 0.0)
+
+
+def _certificate_rel(value: complex, bound: float) -> float:
+    if not _finite_certificate(value, bound):
+        return float("inf")
+    mag = abs(value)
+    if mag == 0.0:
+        return 0.0 if bound == 0.0 else float("inf")
+    return float(bound / mag)
+
+
+def _check_certified_input(A: Any) -> None:
+    try:
+        finite = np.all(np.isfinite(np.asarray(A)))
+    except (TypeError, ValueError):
+        finite = False
+    if not finite:
+        raise ValueError("certified evaluation requires finite input entries")
+
+
+def _certified_batched(func: str, matrices, rtol: float | None):
+    """Certified tier with the proven ladder certified-fp64 -> certified-dd
+    (gbskernels/__init__.py:374-478; the mpmath rung is CPU-only and not here:
+    an element that neither rung certifies to rtol raises FloatingPointError)."""
+    stack = _prepare(func, matrices, "fp64")
+    _check_certified_input(stack)
+    values, bounds = _call_aux(func, stack, "certified")
+    out = values.astype(np.complex128, copy=True)
+    diags = []
+    redo = []
+    for i in range(len(out)):
+        v, e = complex(out[i]), float(bounds[i])
+        valid = _finite_certificate(v, e)
+        rel = _certificate_rel(v, e)
+        if rtol is not None and (not valid or not np.isfinite(rel) or rel > rtol):
+            redo.append(i)
+            diags.append(None)
+        elif not valid:
+            raise FloatingPointError(
+                f"certified {func} batch element {i} refused with a non-finite value or bound")
+        else:
+            d = {"tier": "certified-fp64", "abs_error_bound": e, "rel_error_bound": rel}
+            if rtol is not None:
+                d["escalated"] = False
+            diags.append(d)
+    if redo:
+        sub = np.ascontiguousarray(stack[redo])
+        v2, b2 = _call_aux(func, sub, "dd_certified")
+        for j, i in enumerate(redo):
+            vc, bf = complex(v2[j]), float(b2[j])
+            rel2 = _certificate_rel(vc, bf)
+            if _finite_certificate(vc, bf) and np.isfinite(rel2) and rel2 <= rtol:
+                out[i] = vc
+                diags[i] = {"tier": "certified-dd", "escalated": True, "abs_error_bound": bf,
+                            "rel_error_bound": float(rel2)}
+            else:
+                raise FloatingPointError(
+                    f"certified {func} element {i}: neither the fp64 nor the double-double "
+                    f"certificate reaches rtol={rtol} (the mpmath rung is CPU-only)")
+    return out, diags
+
+
+def _check_diag(precision, return_diagnostics):
+    if return_diagnostics and precision not in ("auto", "certified"):
+        raise ValueError("return_diagnostics=True requires precision='auto' or 'certified'")
+    if precision == "certified" and not return_diagnostics:
+        raise ValueError(
+            "precision='certified' returns its error bound via diagnostics; call with "
+            "return_diagnostics=True (a certificate you cannot see is not a certificate)")
+
+
+def _check_rtol(precision, rtol):
+    if rtol is not None and precision != "certified":
+        raise ValueError("rtol is a certified-tier parameter; it requires precision='certified'")
+    if rtol is not None and (not np.isfinite(rtol) or rtol < 0.0):
+        raise ValueError("rtol must be finite and non-negative")
+
+
+def _dispatch_batched(func, matrices, precision, backend, return_diagnostics=False, rtol=None):
+    _check_diag(precision, return_diagnostics)
+    _check_rtol(precision, rtol)
+    _check_backend(backend)
+    if precision == "auto":
+        return _auto_batched(func, matrices, return_diagnostics)
+    if precision == "certified":
+        return _certified_batched(func, matrices, rtol)
+    stack = _prepare(func, matrices, precision)
+    return _call_uniform(func, stack, precision)
+
+
+def _dispatch_single(func, A, precision, backend, return_diagnostics=False, rtol=None):
+    res = _dispatch_batched(func, np.asarray(A)[None, ...], precision, backend, return_diagnostics, rtol)
+    if isinstance(res, tuple):
+        vals, diags = res
+        return complex(vals[0]), diags[0]
+    return complex(res[0])
+
+
+# ------------------------------------------------------------------ public API
+def perm(A: Any, precision: str = "fp64", backend: str = "gpu", return_diagnostics: bool = False,
+         rtol: float | None = None):
+    """Permanent of a single square matrix ``A``."""
+    return _dispatch_single("perm", A, precision, backend, return_diagnostics, rtol)
+
+
+def perm_batched(matrices: Iterable[Any], precision: str = "fp64", backend: str = "gpu",
+                 return_diagnostics: bool = False, rtol: float | None = None):
+    """Permanents of a (B, n, n) batch -> complex128 vector."""
+    return _dispatch_batched("perm", matrices, precision, backend, return_diagnostics, rtol)
+
+
+def haf(A: Any, precision: str = "fp64", backend: str = "gpu", return_diagnostics: bool = False,
+        rtol: float | None = None):
+    """Hafnian of a single symmetric matrix (diagonal ignored)."""
+    return _dispatch_single("haf", A, precision, backend, return_diagnostics, rtol)
+
+
+def haf_batched(matrices: Iterable[Any], precision: str = "fp64", backend: str = "gpu",
+                return_diagnostics: bool = False, rtol: float | None = None):
+    """Hafnians of a (B, N, N) batch of symmetric matrices -> complex128 vector."""
+    return _dispatch_batched("haf", matrices, precision, backend, return_diagnostics, rtol)
+
+
+def lhaf(A: Any, precision: str = "fp64", backend: str = "gpu", return_diagnostics: bool = False,
+         rtol: float | None = None):
+    """Loop hafnian of a single symmetric matrix (odd N via A (+) [1])."""
+    return _dispatch_single("lhaf", A, precision, backend, return_diagnostics, rtol)
+
+
+def lhaf_batched(matrices: Iterable[Any], precision: str = "fp64", backend: str = "gpu",
+                 return_diagnostics: bool = False, rtol: float | None = None):
+    """Loop hafnians of a (B, N, N) batch -> complex128 vector."""
+    return _dispatch_batched("lhaf", matrices, precision, backend, return_diagnostics, rtol)
+
+
+def tor(O: Any, precision: str = "fp64", backend: str = "gpu", return_diagnostics: bool = False,
+        rtol: float | None = None):
+    """Torontonian of a single 2n x 2n matrix O (xxpp ordering)."""
+    return _dispatch_single("tor", O, precision, backend, return_diagnostics, rtol)
+
+
+def tor_batched(matrices: Iterable[Any], precision: str = "fp64", backend: str = "gpu",
+                return_diagnostics: bool = False, rtol: float | None = None):
+    """Torontonians of a (B, 2n, 2n) batch -> complex128 vector."""
+    return _dispatch_batched("tor", matrices, precision, backend, return_diagnostics, rtol)
+
+
+def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: bool = False):
+    """Single large torontonian of a real (2n, 2n) matrix, 2n <= 64
+    (gbskernels/__init__.py:635-691 contract)."""
+    A = np.asarray(O)
+    if np.iscomplexobj(A):
+        if np.any(np.imag(A) != 0):
+            raise ValueError("tor_single is real-domain only; use tor() for complex O (dim <= 48)")
+        A = np.real(A)
+    M = np.ascontiguousarray(A, dtype=np.float64)
+    if M.ndim != 2 or M.shape[0] != M.shape[1] or M.shape[0] % 2 != 0:
+        raise ValueError(f"tor_single: O must be square with even dimension, got {M.shape}")
+    if M.shape[0] > 64:
+        raise ValueError(f"tor_single: dimension {M.shape[0]} exceeds the cap 64 (n <= 32 modes)")
+    if not np.all(np.isfinite(M)):
+        raise ValueError("tor_single: O must contain only finite binary64 values")
+    if not np.array_equal(M, M.T):
+        raise ValueError("tor_single: O must be exactly symmetric after conversion to binary64")
+    n = M.shape[0] // 2
+    g = min(n, 14) if groups is None else int(groups)
+    if not 0 <= g <= n:
+        raise ValueError(f"groups must be in [0, {n}]")
+    lib = _lib.load()
+    v = np.zeros(1)
+    e = np.zeros(1)
+    if certified or dd:
+        tier = "certified-dd" if dd else "certified-fp64"
+        name = "gbs_tor_single_ddcertified_host" if dd else "gbs_tor_single_certified_host"
+        fn = getattr(lib, name, None)
+        if fn is None:
+            raise RuntimeError(f"tor_single({tier}) is not in this build")
+        _lib.check(fn(_lib.dptr(M), n, g, _lib.dptr(v), _lib.dptr(e)), name)
+        vv, ee = float(v[0]), float(e[0])
+        if not (np.isfinite(vv) and np.isfinite(ee) and ee >= 0.0):
+            raise ValueError("tor_single: off the physical domain or uncertifiable "
+                             "(the bound refuses rather than overclaims)")
+        rel = ee / abs(vv) if vv != 0 else float("inf")
+        return vv, {"tier": tier, "abs_error_bound": ee, "rel_error_bound": rel}
+    fn = getattr(lib, "gbs_tor_recursive_single_host", None)
+    if fn is None:
+        raise RuntimeError("tor_single is not in this build")
+    _lib.check(fn(_lib.dptr(M), n, g, _lib.dptr(v)), "gbs_tor_recursive_single_host")
+    vv = float(v[0])
+    if not np.isfinite(vv):
+        raise ValueError("tor_single: input is off the physical domain (I - O_S not SPD)")
+    return vv
+
+
+def gpu_available() -> bool:
+    """True if libgbs_b200.so loads and a CUDA device is visible."""
+    try:
+        _lib.load()
+    except RuntimeError:
+        return False
+    return _lib.device_count() > 0
+
+
+def gpu_backend_kind() -> str:
+    """'gpu' when the sm_100a library loads and a device is present, else 'none'."""
+    return "gpu" if gpu_available() else "none"
+
+
+# ------------------------------------------------------------------ sessions / ragged batches
+class _ResidentResult:
+    """Device-resident (B,) complex128 result (gbskernels/__init__.py:856-908 contract).
+    Exposes ``__cuda_array_interface__`` so ``torch.as_tensor(r, device='cuda')`` or
+    CuPy consume it without a copy; ``.numpy()`` copies to the host."""
+
+    def __init__(self, ptr: ctypes.POINTER(ctypes.c_double), n: int):
+        self._ptr = ptr
+        self._n = n
+
+    @property
+    def __cuda_array_interface__(self):
+        addr = ctypes.cast(self._ptr, ctypes.c_void_p).value or 0
+        return {"shape": (self._n,), "typestr": "<c16", "data": (addr, False), "version": 3}
+
+    def numpy(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.complex128)
+        if self._n:
+            _lib.check(_lib.load().gbs_dev_to_host(self._ptr, _lib.dptr(out.view(np.float64)), self._n),
+                       "gbs_dev_to_host")
+        return out
+
+    def __len__(self) -> int:
+        return self._n
+
+    def close(self) -> None:
+        if self._ptr:
+            _lib.load().gbs_dev_free(self._ptr)
+            self._ptr = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _as_square_list(matrices: Iterable[Any]) -> list[np.ndarray]:
+    out = []
+    for i, m in enumerate(matrices):
+        a = np.ascontiguousarray(np.asarray(m, dtype=np.complex128))
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise ValueError(f"Workspace: matrix #{i} must be square 2-D; got shape {a.shape}")
+        out.append(a)
+    return out
+
+
+def _pack(mats: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    dims = np.array([m.shape[0] for m in mats], dtype=np.int32)
+    sizes = dims.astype(np.int64) ** 2
+    offsets = np.zeros(len(mats), dtype=np.int64)
+    if len(mats) > 1:
+        offsets[1:] = np.cumsum(sizes)[:-1]
+    buf = np.empty(int(sizes.sum()) if len(mats) else 1, dtype=np.complex128)
+    for m, o, s in zip(mats, offsets, sizes):
+        buf[o:o + s] = m.reshape(-1)
+    return buf, dims, offsets
+
+
+class Workspace:
+    """Device-resident, bucketing session for ragged, sampler-shaped workloads
+    (gbskernels/__init__.py:734-908).  One C++ session (stream, monotonically grown
+    device buffers, pinned staging) serves every call.  A ragged batch runs as ONE
+    persistent launch over a device work queue (``persistent=True``, default) or as
+    one launch per (function, size) bucket (``persistent=False``, the reference's
+    plain per-size path); values are identical either way."""
+
+    def __init__(self, backend: str = "gpu", persistent: bool = True) -> None:
+        if backend not in ("cpu", "gpu"):
+            raise ValueError(f"unknown backend {backend!r}; expected 'cpu' or 'gpu'")
+        self._backend = backend
+        self._persistent = persistent
+        self._session = None
+        self._closed = False
+
+    def __enter__(self) -> "Workspace":
+        _check_backend(self._backend)
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(lib.gbs_session_open(ctypes.byref(h)), "gbs_session_open")
+        self._session = h
+        return self
+
+    def __exit__(self, *exc: Any) -> bool:
+        self.close()
+        return False
+
+    def close(self) -> None:
+        """Release the device-resident session.  Idempotent."""
+        if self._closed:
+            return
+        if self._session is not None:
+            _lib.load().gbs_session_close(self._session)
+        self._session = None
+        self._closed = True
+
+    @property
+    def reallocs(self) -> int:
+        if self._session is None:
+            return 0
+        return int(_lib.load().gbs_session_reallocs(self._session))
+
+    def last_stats(self) -> dict:
+        ms = np.zeros(1)
+        launches = np.zeros(1, dtype=np.int32)
+        items = np.zeros(1, dtype=np.int64)
+        _lib.check(_lib.load().gbs_session_last_stats(self._session, _lib.dptr(ms), _lib.iptr(launches),
+                                                      _lib.llptr(items)), "gbs_session_last_stats")
+        return {"kernel_ms": float(ms[0]), "launches": int(launches[0]), "items": int(items[0])}
+
+    def _require(self):
+        if self._closed:
+            raise RuntimeError("Workspace is closed")
+        if self._session is None:
+            raise RuntimeError("Workspace must be entered (use `with Workspace() as ws:`)")
+
+    def perm_batched(self, matrices, precision: str = "fp64") -> np.ndarray:
+        return self._ragged("perm", matrices, precision)
+
+    def haf_batched(self, matrices, precision: str = "fp64") -> np.ndarray:
+        return self._ragged("haf", matrices, precision)
+
+    def lhaf_batched(self, matrices, precision: str = "fp64") -> np.ndarray:
+        return self._ragged("lhaf", matrices, precision)
+
+    def tor_batched(self, matrices, precision: str = "fp64") -> np.ndarray:
+        return self._ragged("tor", matrices, precision)
+
+    def _ragged(self, func: str, matrices, precision: str) -> np.ndarray:
+        self._require()
+        mats = _as_square_list(matrices)
+        if not mats:
+            return np.empty(0, dtype=np.complex128)
+        if precision == "auto":
+            # per-element auto within uniform buckets (value identical to evaluating alone)
+            out = np.empty(len(mats), dtype=np.complex128)
+            buckets: dict[int, list[int]] = {}
+            for i, a in enumerate(mats):
+                buckets.setdefault(a.shape[0], []).append(i)
+            for d, idxs in buckets.items():
+                try:
+                    res = _auto_batched(func, np.stack([mats[i] for i in idxs]), False)
+                except ValueError as e:
+                    raise ValueError(f"matrix #{idxs[0]} (dim {d}): {e}") from e
+                out[idxs] = res
+            return out
+        for i, a in enumerate(mats):
+            try:
+                _prepare(func, a[None], precision)
+            except ValueError as e:
+                raise ValueError(f"matrix #{i} (dim {a.shape[0]}): {e}") from e
+        return self.evaluate([func] * len(mats), mats, [precision] * len(mats))
+
+    def evaluate(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str],
+                 return_status: bool = False):
+        """Mixed-function, mixed-tier, ragged batch in one persistent launch (or per-size
+        launches when the Workspace was opened with persistent=False)."""
+        self._require()
+        B = len(mats)
+        out = np.empty(B, dtype=np.complex128)
+        st = np.zeros(B, dtype=np.int32)
+        aux = np.zeros(B, dtype=np.float64)
+        if B == 0:
+            return (out, st) if return_status else out
+        buf, dims, offs = _pack(mats)
+        fns = np.array([_FN[f] for f in funcs], dtype=np.int32)
+        tiers = np.array([_TIER[p] for p in precisions], dtype=np.int32)
+        rc = _lib.load().gbs_queue_evaluate(
+            self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims), _lib.llptr(offs),
+            _lib.dptr(buf.view(np.float64)), 0 if self._persistent else 1,
+            _lib.dptr(out.view(np.float64)), _lib.dptr(aux), _lib.iptr(st))
+        _lib.check(rc, "gbs_queue_evaluate")
+        return (out, st) if return_status else out
+
+    # device-resident outputs (uniform batches)
+    def perm_resident(self, matrices, precision: str = "fp64"):
+        return self._resident("perm", matrices, precision)
+
+    def haf_resident(self, matrices, precision: str = "fp64"):
+        return self._resident("haf", matrices, precision)
+
+    def lhaf_resident(self, matrices, precision: str = "fp64"):
+        return self._resident("lhaf", matrices, precision)
+
+    def tor_resident(self, matrices, precision: str = "fp64"):
+        return self._resident("tor", matrices, precision)
+
+    def _resident(self, func: str, matrices, precision: str):
+        self._require()
+        if precision != "fp64":
+            raise NotImplementedError("device-resident output is fp64 only; use precision='fp64'")
+        try:
+            stack = np.ascontiguousarray(np.asarray(matrices, dtype=np.complex128))
+            uniform = stack.ndim == 3
+        except (ValueError, TypeError):
+            uniform = False
+        if not uniform:
+            raise ValueError("device-resident output needs a uniform (B, d, d) batch")
+        stack = _prepare(func, stack, precision)
+        B, d = stack.shape[0], stack.shape[1]
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        rc = _lib.load().gbs_session_evaluate_resident(self._session, _FN[func], 0,
+                                                       _lib.dptr(stack.view(np.float64)), d, B,
+                                                       ctypes.byref(ptr))
+        _lib.check(rc, "gbs_session_evaluate_resident")
+        return _ResidentResult(ptr, B)
+
+
+def queue_evaluate(funcs: list[str], mats: list[np.ndarray], precisions: list[str] | None = None,
+                   persistent: bool = True) -> np.ndarray:
+    """One-shot mixed batch (functions, sizes and fp64/dd tiers mixed) through a
+    temporary Workspace."""
+    precisions = precisions or ["fp64"] * len(mats)
+    with Workspace(persistent=persistent) as ws:
+        return ws.evaluate(funcs, [np.asarray(m, dtype=np.complex128) for m in mats], precisions)

@@ -1,0 +1,280 @@
+// gbs_items.cuh -- the work-item kernel behind every batched evaluation.
+//
+// One kernel template serves the plain per-size launches (a single (function,
+// tier) branch compiled in, lean registers) and the persistent mixed-size queue
+// (several branches compiled in): warps pull work items from a device queue head
+// with one atomic each, evaluate, publish a partial, and the warp that finishes
+// the last item of an instance reduces that instance's partials in item order.
+// No warp ever waits on another, so there is no spin anywhere in the kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "gbs_common.cuh"
+#include "gbs_kernels.cuh"
+#include "haf_dd.cuh"
+#include "haf_pt.cuh"
+#include "perm_tor.cuh"
+
+namespace gbsb {
+
+constexpr int kTorBatchMaxModes = 24;  // batched torontonian cap (dim 48)
+constexpr int kTorPackedMax = (2 * kTorBatchMaxModes) * (2 * kTorBatchMaxModes + 1) / 2;
+
+// ------------------------------------------------------------------ item evaluators
+struct ItemResult {
+  ddc val;
+  double aux;
+  int st;
+};
+
+__device__ __forceinline__ ddc ddc_from_c(cplx v) { return ddc{dd_make(v.re), dd_make(v.im)}; }
+
+// Permanent item: Gray indices [lo, lo + count), 32 lanes x R = count / 32 each
+// (count < 32 only when the whole walk is shorter than a warp).
+template <int NN, int TIER>
+__device__ ItemResult perm_item_n(const double* A2, unsigned long long lo, unsigned long long count, int lane) {
+  ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStOk};
+  unsigned long long R = count >= 32 ? count / 32 : 1;
+  bool active = count >= 32 || (unsigned long long)lane < count;
+  unsigned long long i0 = lo + (unsigned long long)lane * R;
+  if (TIER == kTierDD) {
+    ddc v = ddc{dd_make(0.0), dd_make(0.0)};
+    if (active) v = perm_lane_range_dd<NN>(A2, i0, R);
+    r.val = warp_sum_ddc(v);
+  } else {
+    double absacc = 0.0;
+    cplx v = mkc(0.0, 0.0);
+    if (active) v = perm_lane_range<NN, TIER == kTierKappa>(A2, i0, R, absacc);
+    v = warp_sum_c(v);
+    r.val = ddc_from_c(v);
+    if (TIER == kTierKappa) r.aux = warp_sum_d(absacc);
+  }
+  return r;
+}
+
+template <int TIER>
+__device__ ItemResult perm_item(const double* __restrict__ mats, const InstDesc& d, const WorkItem& w,
+                                double* ws, int lane) {
+  const int n = d.dim;
+  const double* A = mats + d.off;
+  // stage 2A (exact scaling) in this warp's shared workspace
+  for (int e = lane; e < n * n; e += 32) st_c(ws + e * 2, cscale(ld_c(A + e * 2), 2.0));
+  __syncwarp();
+  ItemResult r;
+  switch (n) {
+#define GBSB_PERM_CASE(K) \
+  case K: r = perm_item_n<K, TIER>(ws, w.lo, w.count, lane); break;
+    GBSB_PERM_CASE(1) GBSB_PERM_CASE(2) GBSB_PERM_CASE(3) GBSB_PERM_CASE(4) GBSB_PERM_CASE(5)
+    GBSB_PERM_CASE(6) GBSB_PERM_CASE(7) GBSB_PERM_CASE(8) GBSB_PERM_CASE(9) GBSB_PERM_CASE(10)
+    GBSB_PERM_CASE(11) GBSB_PERM_CASE(12) GBSB_PERM_CASE(13) GBSB_PERM_CASE(14) GBSB_PERM_CASE(15)
+    GBSB_PERM_CASE(16) GBSB_PERM_CASE(17) GBSB_PERM_CASE(18) GBSB_PERM_CASE(19) GBSB_PERM_CASE(20)
+    GBSB_PERM_CASE(21) GBSB_PERM_CASE(22) GBSB_PERM_CASE(23) GBSB_PERM_CASE(24) GBSB_PERM_CASE(25)
+    GBSB_PERM_CASE(26) GBSB_PERM_CASE(27) GBSB_PERM_CASE(28)
+#undef GBSB_PERM_CASE
+    default:
+      r = ItemResult{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStTooLarge};
+  }
+  __syncwarp();
+  return r;
+}
+
+template <int TIER>
+__device__ ItemResult haf_item(const double* __restrict__ mats, const InstDesc& d, const WorkItem& w,
+                               bool loop, double* ws, int haf_smax, int lane) {
+  ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStOk};
+  const int N = d.dim, n = N / 2;
+  const double* A = mats + d.off;
+  if (TIER == kTierDD) {
+    const HafDDLayout L = haf_dd_layout(haf_smax);
+    ddc acc = ddc{dd_make(0.0), dd_make(0.0)};
+    for (unsigned long long k = 0; k < w.count; ++k) {
+      ddc t = haf_subset_term_dd(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      acc = ddc_add(acc, t);
+    }
+    r.val = acc;
+  } else {
+    const HafLayout L = haf_layout(haf_smax);
+    cplx acc = mkc(0.0, 0.0);
+    double absacc = 0.0;
+    for (unsigned long long k = 0; k < w.count; ++k) {
+      cplx t = haf_subset_term_tc(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      acc = cadd(acc, t);
+      if (TIER == kTierKappa) absacc += cabs_fast(t);
+    }
+    r.val = ddc_from_c(acc);
+    r.aux = absacc;
+  }
+  return r;
+}
+
+template <int TIER>
+__device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& d, const WorkItem& w,
+                               double* ws, int lane) {
+  ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStOk};
+  const int n = d.dim / 2;
+  const int dim = d.dim;
+  // stage the real part of O in this warp's shared workspace (row-major doubles)
+  const double* Oc = mats + d.off;
+  for (int e = lane; e < dim * dim; e += 32) ws[e] = Oc[2 * e];
+  __syncwarp();
+  const bool active = (unsigned long long)lane < w.count;
+  const uint32_t pat = (uint32_t)(w.lo + lane);
+  bool ok = true;
+  double absacc = 0.0;
+  if (TIER == kTierDD) {
+    dd total = dd_make(0.0);
+    if (active) {
+      dd L[kTorPackedMax];
+      ok = tor_lane_subtree<dd>(ws, n, d.param, pat, L, total, absacc, false);
+    }
+    dd v = ok ? total : dd_make(0.0);
+    ddc c = ddc{v, dd_make(0.0)};
+    c = warp_sum_ddc(c);
+    r.val = c;
+  } else {
+    double total = 0.0;
+    if (active) {
+      double L[kTorPackedMax];
+      ok = tor_lane_subtree<double>(ws, n, d.param, pat, L, total, absacc, TIER == kTierKappa);
+    }
+    double v = warp_sum_d(ok ? total : 0.0);
+    r.val = ddc{dd_make(v), dd_make(0.0)};
+    r.aux = warp_sum_d(absacc);
+  }
+  const bool all_ok = __all_sync(0xffffffffu, ok);
+  if (!all_ok) r.st = kStOffDomain;
+  __syncwarp();
+  return r;
+}
+
+// ------------------------------------------------------------------ the item kernel
+template <unsigned BR>
+__device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstDesc& d, const WorkItem& w,
+                                                double* ws, int lane) {
+  ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStTooLarge};
+  switch (d.ft) {
+#define GBSB_BR(FN, TIER, CALL) \
+  case ft_code(FN, TIER):         \
+    if constexpr ((BR >> ft_code(FN, TIER)) & 1u) { r = CALL; } \
+    break;
+    GBSB_BR(kFnPerm, kTierFp64, (perm_item<kTierFp64>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnPerm, kTierKappa, (perm_item<kTierKappa>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnPerm, kTierDD, (perm_item<kTierDD>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnHaf, kTierFp64, (haf_item<kTierFp64>(P.mats, d, w, false, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnHaf, kTierKappa, (haf_item<kTierKappa>(P.mats, d, w, false, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnHaf, kTierDD, (haf_item<kTierDD>(P.mats, d, w, false, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnLhaf, kTierFp64, (haf_item<kTierFp64>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnLhaf, kTierKappa, (haf_item<kTierKappa>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnLhaf, kTierDD, (haf_item<kTierDD>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnTor, kTierFp64, (tor_item<kTierFp64>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnTor, kTierKappa, (tor_item<kTierKappa>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnTor, kTierDD, (tor_item<kTierDD>(P.mats, d, w, ws, lane)))
+#undef GBSB_BR
+    default:
+      break;
+  }
+  return r;
+}
+
+template <unsigned BR>
+__global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
+  extern __shared__ __align__(128) double smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  double* ws = smem + (size_t)warp * P.ws_doubles;
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(P.head, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= P.n_items) break;
+    if (P.order) it = P.order[it];
+    const WorkItem w = P.items[it];
+    const InstDesc d = P.insts[w.inst];
+    ItemResult r = eval_item<BR>(P, d, w, ws, lane);
+    int last = 0;
+    if (lane == 0) {
+      double4 pv = make_double4(r.val.re.hi, r.val.re.lo, r.val.im.hi, r.val.im.lo);
+      *reinterpret_cast<double4*>(P.part + (size_t)it * 4) = pv;
+      P.paux[it] = r.aux;
+      P.pst[it] = r.st;
+      __threadfence();
+      const int old = atomicAdd(P.done + w.inst, 1);
+      last = (old == d.nitems - 1);
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+      __threadfence();
+      // Deterministic reduction: lane l sums items l, l+32, ... in order, then a
+      // fixed butterfly combines the lanes.  Partials are read through L2.
+      ddc acc = ddc{dd_make(0.0), dd_make(0.0)};
+      double aux = 0.0;
+      int st = kStOk;
+      for (int k = lane; k < d.nitems; k += 32) {
+        const double* pp = P.part + (size_t)(d.item0 + k) * 4;
+        ddc v = ddc{dd{__ldcg(pp), __ldcg(pp + 1)}, dd{__ldcg(pp + 2), __ldcg(pp + 3)}};
+        acc = ddc_add(acc, v);
+        aux += __ldcg(P.paux + d.item0 + k);
+        st = max(st, __ldcg(P.pst + d.item0 + k));
+      }
+      acc = warp_sum_ddc(acc);
+      aux = warp_sum_d(aux);
+#pragma unroll
+      for (int m = 16; m > 0; m >>= 1) st = max(st, __shfl_xor_sync(0xffffffffu, st, m));
+      if (lane == 0) {
+        cplx v = ddc_to_c(acc);
+        const int fn = d.ft >> 2;
+        if (fn == kFnPerm && d.dim > 0) {
+          const double sc = ldexp(1.0, -(d.dim - 1));  // 1 / 2^(n-1), exact
+          v = cscale(v, sc);
+          aux *= sc;
+        }
+        if (st == kStOffDomain) v = mkc(NAN, NAN);
+        P.out[2 * (size_t)w.inst] = v.re;
+        P.out[2 * (size_t)w.inst + 1] = v.im;
+        P.aux_out[w.inst] = aux;
+        P.st_out[w.inst] = st;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ launch helpers
+template <unsigned BR>
+static cudaError_t launch_br(const ItemLaunch& P, int grid, int warps, cudaStream_t stream) {
+  const size_t smem = (size_t)warps * P.ws_doubles * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(gbs_items_kernel<BR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  gbs_items_kernel<BR><<<grid, warps * 32, smem, stream>>>(P);
+  return cudaGetLastError();
+}
+
+template <unsigned BR>
+static int occ_br(const ItemLaunch& P, int warps) {
+  const size_t smem = (size_t)warps * P.ws_doubles * sizeof(double);
+  if (cudaFuncSetAttribute(gbs_items_kernel<BR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return 0;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, gbs_items_kernel<BR>, warps * 32, smem) != cudaSuccess)
+    return 0;
+  return nb;
+}
+
+// One translation unit per group of branch sets (parallel builds): each defines
+//   bool items_launch_<group>(unsigned br, const ItemLaunch&, int grid, int warps, cudaStream_t, cudaError_t*)
+//   int  items_occ_<group>(unsigned br, const ItemLaunch&, int warps)        (-1: not in group)
+#define GBSB_DEFINE_GROUP(NAME, LIST)                                                              \
+  bool items_launch_##NAME(unsigned br, const ItemLaunch& P, int grid, int warps, cudaStream_t s,    \
+                           cudaError_t* err) {                                                       \
+    switch (br) { LIST(GBSB_LCASE) default: return false; }                                          \
+  }                                                                                                  \
+  int items_occ_##NAME(unsigned br, const ItemLaunch& P, int warps) {                                \
+    switch (br) { LIST(GBSB_OCASE) default: return -1; }                                             \
+  }
+#define GBSB_LCASE(B) \
+  case (unsigned)(B): *err = launch_br<(B)>(P, grid, warps, s); return true;
+#define GBSB_OCASE(B) \
+  case (unsigned)(B): return occ_br<(B)>(P, warps);
+
+}  // namespace gbsb

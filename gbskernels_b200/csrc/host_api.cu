@@ -1,0 +1,710 @@
+// host_api.cu -- the C++ host runtime and the C ABI of libgbs_b200.so.
+//
+// Layers (each replaces a reference component; citations are to the reference):
+//   * planner: cuts every instance into work items (function of (func, tier, size)
+//     only, so values are independent of batch composition);
+//   * session: stream + monotonically growing device buffers + pinned staging
+//     (core/host_api.cu:474-648, gbs_session_*), one H2D of the packed batch, one
+//     launch, one D2H;
+//   * bucketing: the ragged "plain per-size launch" path, one launch per
+//     (func, tier, size) bucket (gbskernels/__init__.py:813-852 Workspace._ragged);
+//   * persistent mixed queue: ONE launch over all instances of a ragged, mixed
+//     function / tier batch, work items ordered heaviest first (new);
+//   * tier logic: auto = fp64 + sum|term| indicator, device double-double rerun of
+//     the elements with kappa >= 1e8 (gbskernels/__init__.py:240-297, without the
+//     reference's CPU mpmath fallback);
+//   * C ABI: gbs_*_host, gbs_session_*, gbs_queue_* (include/gbs_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gbs_kernels.cuh"
+#include "haf_dd.cuh"
+#include "haf_pt.cuh"
+
+namespace gbsb {
+
+// kernel groups (k_*.cu)
+#define GBSB_DECL_GROUP(NAME)                                                                       \
+  bool items_launch_##NAME(unsigned br, const ItemLaunch& P, int grid, int warps, cudaStream_t s,   \
+                           cudaError_t* err);                                                       \
+  int items_occ_##NAME(unsigned br, const ItemLaunch& P, int warps);
+GBSB_DECL_GROUP(perm_fp64)
+GBSB_DECL_GROUP(perm_kappa)
+GBSB_DECL_GROUP(perm_dd)
+GBSB_DECL_GROUP(haf)
+GBSB_DECL_GROUP(haf_dd)
+GBSB_DECL_GROUP(tor)
+GBSB_DECL_GROUP(mixed)
+#undef GBSB_DECL_GROUP
+
+static cudaError_t launch_any(unsigned br, const ItemLaunch& P, int grid, int warps, cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  if (items_launch_perm_fp64(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_perm_kappa(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_perm_dd(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_haf(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_haf_dd(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_tor(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_mixed(br, P, grid, warps, s, &e)) return e;
+  return cudaErrorInvalidValue;
+}
+static int occ_any(unsigned br, const ItemLaunch& P, int warps) {
+  int r;
+  if ((r = items_occ_perm_fp64(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_perm_kappa(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_perm_dd(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_haf(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_haf_dd(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_tor(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_mixed(br, P, warps)) >= 0) return r;
+  return 0;
+}
+// Smallest compiled branch set covering `need`.
+static unsigned cover(unsigned need) {
+  if (__builtin_popcount(need) == 1) return need;
+  const unsigned sets[] = {kBrHafLhafFp64, kBrServe, kBrMixed};
+  for (unsigned s : sets)
+    if ((s & need) == need) return s;
+  return 0;  // not coverable by one launch (the caller splits)
+}
+
+// ------------------------------------------------------------------ caps
+constexpr int kPermCap = 28;
+constexpr int kHafCap = kHafMaxN;   // 32 (after odd-N loop augmentation)
+constexpr int kTorCapModes = 24;
+
+// ------------------------------------------------------------------ requests and plans
+struct Req {
+  int fn, tier;
+  int dim;              // matrix side as given by the caller (tor: 2n)
+  const double* mat;    // complex interleaved, row-major
+};
+
+struct Plan {
+  std::vector<InstDesc> insts;
+  std::vector<WorkItem> items;
+  std::vector<int> order;
+  std::vector<int> trivial;      // instances answered on the host (size-0 / odd haf)
+  std::vector<cplx> trivial_val;
+  unsigned need = 0;
+  int haf_smax = 2;
+  int ws_doubles = 0;
+  long long mat_doubles = 0;
+  double cost = 0.0;
+};
+
+
+// Cost model (relative units) used only to order the queue heaviest-first.
+static double item_cost(int fn, int dim, unsigned long long count, int tier) {
+  double c;
+  switch (fn) {
+    case kFnPerm: c = (double)count * dim; break;
+    case kFnTor: { int n = dim / 2; c = (double)count * std::ldexp(1.0, n) * n * n / 32.0; break; }
+    default: { double n = dim / 2.0; c = (double)count * (n + 1) * n * n * n; break; }
+  }
+  return tier == kTierDD ? 20.0 * c : c;
+}
+
+// Append one instance (already validated) to the plan.  Returns the instance index.
+static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, long long off) {
+  InstDesc d{};
+  d.off = off;
+  d.dim = dim_eval;
+  d.ft = ft_code(fn, tier);
+  d.item0 = (int)P.items.size();
+  d.param = 0;
+  d.real_in = real_in ? 1 : 0;
+  const int idx = (int)P.insts.size();
+  auto add = [&](unsigned long long lo, unsigned long long count) {
+    WorkItem w{};
+    w.inst = idx;
+    w.lo = lo;
+    w.count = count;
+    P.items.push_back(w);
+  };
+  if (fn == kFnPerm) {
+    const int n = dim_eval;
+    const unsigned long long terms = 1ull << (n - 1);
+    if (terms <= 32) {
+      add(0, terms);
+    } else {
+      const int rcap = tier == kTierDD ? 6 : 10;
+      const int rlog = std::min(n - 1 - 5, rcap);
+      const unsigned long long cnt = 32ull << rlog;
+      for (unsigned long long lo = 0; lo < terms; lo += cnt) add(lo, cnt);
+      d.param = rlog;
+    }
+  } else if (fn == kFnHaf || fn == kFnLhaf) {
+    const int n = dim_eval / 2;
+    const unsigned long long masks = 1ull << n;
+    const int per = tier == kTierDD ? std::max(0, n - 9) : std::max(0, n - 7);
+    const unsigned long long cnt = 1ull << per;
+    for (unsigned long long lo = 0; lo < masks; lo += cnt) add(lo, std::min(cnt, masks - lo));
+    P.haf_smax = std::max(P.haf_smax, dim_eval);
+  } else {  // tor
+    const int n = dim_eval / 2;
+    const int rcap = tier == kTierDD ? 7 : 10;
+    const int g = std::max(std::min(n, 5), n - rcap);
+    const unsigned long long pats = 1ull << g;
+    for (unsigned long long lo = 0; lo < pats; lo += 32) add(lo, std::min<unsigned long long>(32, pats - lo));
+    d.param = g;
+  }
+  d.nitems = (int)P.items.size() - d.item0;
+  P.insts.push_back(d);
+  P.need |= 1u << d.ft;
+  return idx;
+}
+
+static int ws_for_plan(const Plan& P) {
+  int ws = 2;
+  for (const InstDesc& d : P.insts) {
+    const int fn = d.ft >> 2, tier = d.ft & 3;
+    int w = 0;
+    if (fn == kFnPerm) w = 2 * d.dim * d.dim;
+    else if (fn == kFnTor) w = d.dim * d.dim;
+    else w = tier == kTierDD ? haf_dd_layout(P.haf_smax).total : haf_layout(P.haf_smax).total;
+    ws = std::max(ws, w);
+  }
+  return (ws + 3) & ~3;  // 32-byte multiple per warp
+}
+
+// ------------------------------------------------------------------ session
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+struct PinBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace gbsb
+
+struct gbs_session {
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int sms = 148;
+  gbsb::DevBuf mats, meta, part, paux, pst, done, head, out, aux, st;
+  gbsb::PinBuf pin_in, pin_meta, pin_out;
+  size_t reallocs = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_kernel_ms = 0.f;
+  int last_launches = 0;
+  long long last_items = 0;
+  std::mutex mu;
+};
+
+namespace gbsb {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+static cudaError_t grow_dev(DevBuf& b, size_t bytes, size_t* reallocs) {
+  if (bytes <= b.cap) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  size_t want = std::max(bytes, (size_t)256);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e == cudaSuccess) {
+    b.cap = want;
+    if (reallocs) ++*reallocs;
+  }
+  return e;
+}
+static cudaError_t grow_pin(PinBuf& b, size_t bytes) {
+  if (bytes <= b.cap) return cudaSuccess;
+  if (b.p) cudaFreeHost(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  size_t want = std::max(bytes, (size_t)256);
+  cudaError_t e = cudaMallocHost(&b.p, want);
+  if (e == cudaSuccess) b.cap = want;
+  return e;
+}
+
+// Validate + normalise one request.  Returns 0 or an error code; on success fills
+// the evaluated side length (odd loop hafnian augmented) and the real-input flag.
+static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, cplx* tval) {
+  *trivial = false;
+  *real_in = false;
+  if (r.dim < 0) return fail(cudaErrorInvalidValue, "negative matrix dimension");
+  if (r.tier < 0 || r.tier > 2) return fail(cudaErrorInvalidValue, "unsupported precision tier");
+  switch (r.fn) {
+    case kFnPerm:
+      if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
+      if (r.dim > kPermCap) return fail(cudaErrorInvalidValue, "permanent: n above the cap 28");
+      *dim_eval = r.dim;
+      return 0;
+    case kFnHaf:
+      if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
+      if (r.dim & 1) { *trivial = true; *tval = mkc(0, 0); return 0; }
+      if (r.dim > kHafCap) return fail(cudaErrorInvalidValue, "hafnian: N above the cap 32");
+      *dim_eval = r.dim;
+      return 0;
+    case kFnLhaf: {
+      if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
+      int d = r.dim + (r.dim & 1);  // lhaf(A) = lhaf(A (+) [1]) for odd N
+      if (d > kHafCap) return fail(cudaErrorInvalidValue, "loop hafnian: N above the cap 32");
+      *dim_eval = d;
+      return 0;
+    }
+    case kFnTor: {
+      if (r.dim & 1) return fail(cudaErrorInvalidValue, "torontonian: matrix side must be even");
+      if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
+      if (r.dim / 2 > kTorCapModes) return fail(cudaErrorInvalidValue, "torontonian: modes above the cap 24");
+      bool re = true;
+      const size_t nn = (size_t)r.dim * r.dim;
+      for (size_t i = 0; i < nn; ++i)
+        if (r.mat[2 * i + 1] != 0.0) { re = false; break; }
+      if (!re) return fail(cudaErrorNotSupported, "torontonian: complex O is not supported by the batched kernel");
+      *real_in = true;
+      *dim_eval = r.dim;
+      return 0;
+    }
+    default:
+      return fail(cudaErrorInvalidValue, "unknown function code");
+  }
+}
+
+struct RunOpts {
+  bool per_size = false;   // one launch per (func, tier, size) bucket
+  bool sort_heavy = true;  // heaviest instances first in the queue
+  int warps = 4;           // warps per block
+};
+
+// Core: evaluate `reqs` on the session stream.  out: 2 doubles per request, aux: 1
+// double per request (sum |term|, kappa tier), st: status per request.
+static int run_batch(gbs_session* s, const std::vector<Req>& reqs, double* out, double* aux, int* st,
+                     const RunOpts& opt) {
+  const int B = (int)reqs.size();
+  if (B == 0) return 0;
+  // ---- validate & size
+  std::vector<int> dim_eval(B, 0);
+  std::vector<char> real_in(B, 0), trivial(B, 0);
+  std::vector<cplx> tval(B);
+  long long mat_doubles = 0;
+  for (int i = 0; i < B; ++i) {
+    bool re = false, tr = false;
+    int rc = check_req(reqs[i], &dim_eval[i], &re, &tr, &tval[i]);
+    if (rc) {
+      g_last_error = "request #" + std::to_string(i) + ": " + g_last_error;
+      return rc;
+    }
+    real_in[i] = re;
+    trivial[i] = tr;
+    if (!tr) mat_doubles += 2ll * dim_eval[i] * dim_eval[i];
+  }
+  // ---- group (per-size) or single queue
+  std::vector<std::vector<int>> groups;
+  if (opt.per_size) {
+    std::vector<long long> keys;
+    for (int i = 0; i < B; ++i) {
+      if (trivial[i]) continue;
+      long long key = ((long long)reqs[i].fn * 8 + reqs[i].tier) * 4096 + dim_eval[i];
+      size_t g = std::find(keys.begin(), keys.end(), key) - keys.begin();
+      if (g == keys.size()) { keys.push_back(key); groups.emplace_back(); }
+      groups[g].push_back(i);
+    }
+  } else {
+    // one persistent launch for every haf / lhaf / tor request; the permanent runs
+    // its own queue (one per tier) because its register budget differs
+    groups.resize(4);
+    for (int i = 0; i < B; ++i) {
+      if (trivial[i]) continue;
+      groups[reqs[i].fn == kFnPerm ? 1 + reqs[i].tier : 0].push_back(i);
+    }
+  }
+  // ---- upload every matrix once (pinned staging, one H2D)
+  cudaError_t e = grow_pin(s->pin_in, std::max<long long>(mat_doubles, 2) * sizeof(double));
+  if (e == cudaSuccess) e = grow_dev(s->mats, std::max<long long>(mat_doubles, 2) * sizeof(double), &s->reallocs);
+  if (e != cudaSuccess) return fail(e, "allocating matrix buffers");
+  std::vector<long long> off(B, 0);
+  {
+    double* dst = (double*)s->pin_in.p;
+    long long o = 0;
+    for (int i = 0; i < B; ++i) {
+      if (trivial[i]) continue;
+      off[i] = o;
+      const int d = reqs[i].dim, de = dim_eval[i];
+      if (de == d) {
+        std::memcpy(dst + o, reqs[i].mat, sizeof(double) * 2 * (size_t)d * d);
+      } else {  // odd loop hafnian: A (+) [1]
+        std::memset(dst + o, 0, sizeof(double) * 2 * (size_t)de * de);
+        for (int r = 0; r < d; ++r)
+          std::memcpy(dst + o + 2ll * r * de, reqs[i].mat + 2ll * r * d, sizeof(double) * 2 * d);
+        dst[o + 2ll * ((long long)d * de + d)] = 1.0;
+      }
+      o += 2ll * de * de;
+    }
+  }
+  if (mat_doubles > 0) {
+    e = cudaMemcpyAsync(s->mats.p, s->pin_in.p, mat_doubles * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return fail(e, "uploading matrices");
+  }
+  s->last_launches = 0;
+  s->last_items = 0;
+  float kernel_ms = 0.f;
+  // ---- one launch per group
+  for (const std::vector<int>& grp : groups) {
+    if (grp.empty()) continue;
+    Plan P;
+    for (int i : grp) plan_instance(P, reqs[i].fn, reqs[i].tier, dim_eval[i], real_in[i], off[i]);
+    P.ws_doubles = ws_for_plan(P);
+    const int ni = (int)P.insts.size(), nit = (int)P.items.size();
+    // queue order: instances heaviest first (items of one instance stay contiguous)
+    std::vector<int> inst_order(ni);
+    for (int k = 0; k < ni; ++k) inst_order[k] = k;
+    if (opt.sort_heavy && !opt.per_size) {
+      std::vector<double> c(ni);
+      for (int k = 0; k < ni; ++k) {
+        const InstDesc& d = P.insts[k];
+        c[k] = item_cost(d.ft >> 2, d.dim, P.items[d.item0].count, d.ft & 3);
+      }
+      std::stable_sort(inst_order.begin(), inst_order.end(), [&](int a, int b) { return c[a] > c[b]; });
+    }
+    P.order.reserve(nit);
+    for (int k : inst_order)
+      for (int j = 0; j < P.insts[k].nitems; ++j) P.order.push_back(P.insts[k].item0 + j);
+    unsigned br = cover(P.need);
+    if (br == 0) return fail(cudaErrorNotSupported, "batch mixes the permanent with other functions");
+    // ---- buffers
+    const size_t meta_bytes = ni * sizeof(InstDesc) + nit * sizeof(WorkItem) + nit * sizeof(int);
+    e = grow_pin(s->pin_meta, meta_bytes);
+    if (e == cudaSuccess) e = grow_dev(s->meta, meta_bytes, &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->part, (size_t)nit * 4 * sizeof(double), &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->paux, (size_t)nit * sizeof(double), &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->pst, (size_t)nit * sizeof(int), &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->done, (size_t)ni * sizeof(int), &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->head, 16, &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->out, (size_t)ni * 2 * sizeof(double), &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->aux, (size_t)ni * sizeof(double), &s->reallocs);
+    if (e == cudaSuccess) e = grow_dev(s->st, (size_t)ni * sizeof(int), &s->reallocs);
+    if (e == cudaSuccess) e = grow_pin(s->pin_out, (size_t)ni * (3 * sizeof(double) + sizeof(int)));
+    if (e != cudaSuccess) return fail(e, "allocating work buffers");
+    // the meta upload must not overwrite staging still in flight from a previous group
+    e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(e, "synchronising before upload");
+    char* pm = (char*)s->pin_meta.p;
+    std::memcpy(pm, P.insts.data(), ni * sizeof(InstDesc));
+    std::memcpy(pm + ni * sizeof(InstDesc), P.items.data(), nit * sizeof(WorkItem));
+    std::memcpy(pm + ni * sizeof(InstDesc) + nit * sizeof(WorkItem), P.order.data(), nit * sizeof(int));
+    e = cudaMemcpyAsync(s->meta.p, pm, meta_bytes, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->head.p, 0, 16, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->done.p, 0, (size_t)ni * sizeof(int), s->stream);
+    if (e != cudaSuccess) return fail(e, "uploading the work queue");
+    ItemLaunch L{};
+    L.mats = (const double*)s->mats.p;
+    L.insts = (const InstDesc*)s->meta.p;
+    L.items = (const WorkItem*)((char*)s->meta.p + ni * sizeof(InstDesc));
+    L.order = (const int*)((char*)s->meta.p + ni * sizeof(InstDesc) + nit * sizeof(WorkItem));
+    L.n_items = nit;
+    L.head = (int*)s->head.p;
+    L.done = (int*)s->done.p;
+    L.part = (double*)s->part.p;
+    L.paux = (double*)s->paux.p;
+    L.pst = (int*)s->pst.p;
+    L.out = (double*)s->out.p;
+    L.aux_out = (double*)s->aux.p;
+    L.st_out = (int*)s->st.p;
+    L.ws_doubles = P.ws_doubles;
+    L.haf_smax = P.haf_smax;
+    int warps = opt.warps;
+    const size_t smem_per_warp = (size_t)P.ws_doubles * sizeof(double);
+    while (warps > 1 && (size_t)warps * smem_per_warp > 200 * 1024) warps >>= 1;
+    int bps = occ_any(br, L, warps);
+    if (bps <= 0) return fail(cudaErrorInvalidConfiguration, "work item kernel does not fit on an SM");
+    long long want_blocks = (nit + warps - 1) / warps;
+    int grid = (int)std::min<long long>((long long)s->sms * bps, want_blocks);
+    cudaEventRecord(s->ev0, s->stream);
+    e = launch_any(br, L, grid, warps, s->stream);
+    cudaEventRecord(s->ev1, s->stream);
+    if (e != cudaSuccess) return fail(e, "launching the work item kernel");
+    // ---- results
+    double* po = (double*)s->pin_out.p;
+    double* pa = po + 2 * ni;
+    int* ps = (int*)(pa + ni);
+    e = cudaMemcpyAsync(po, s->out.p, (size_t)ni * 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pa, s->aux.p, (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ps, s->st.p, (size_t)ni * sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(e, "evaluating the batch");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    kernel_ms += ms;
+    s->last_launches += 1;
+    s->last_items += nit;
+    for (int k = 0; k < ni; ++k) {
+      const int i = grp[k];
+      out[2 * i] = po[2 * k];
+      out[2 * i + 1] = po[2 * k + 1];
+      if (aux) aux[i] = pa[k];
+      if (st) st[i] = ps[k];
+    }
+  }
+  s->last_kernel_ms = kernel_ms;
+  for (int i = 0; i < B; ++i) {
+    if (!trivial[i]) continue;
+    out[2 * i] = tval[i].re;
+    out[2 * i + 1] = tval[i].im;
+    if (aux) aux[i] = std::hypot(tval[i].re, tval[i].im);
+    if (st) st[i] = kStOk;
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------ process-wide default session
+static std::mutex g_default_mu;
+static gbs_session* g_default = nullptr;
+
+static int session_open(gbs_session** out) {
+  gbs_session* s = new gbs_session();
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
+  if (e != cudaSuccess) {
+    delete s;
+    *out = nullptr;
+    return fail(e, "opening a session");
+  }
+  *out = s;
+  return 0;
+}
+
+static void session_free(gbs_session* s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (DevBuf* b : {&s->mats, &s->meta, &s->part, &s->paux, &s->pst, &s->done, &s->head, &s->out, &s->aux, &s->st})
+    if (b->p) cudaFree(b->p);
+  for (PinBuf* b : {&s->pin_in, &s->pin_meta, &s->pin_out})
+    if (b->p) cudaFreeHost(b->p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+static int with_default(gbs_session** s) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default) {
+    int rc = session_open(&g_default);
+    if (rc) return rc;
+  }
+  *s = g_default;
+  return 0;
+}
+
+// Uniform (B, d, d) batch through a session.
+static int uniform(gbs_session* s, int fn, int tier, const double* m, int dim, int b, double* o, double* aux,
+                   int* st) {
+  if (b <= 0) return 0;
+  if (!m || !o) return fail(cudaErrorInvalidValue, "null buffer");
+  std::vector<Req> reqs(b);
+  const size_t stride = 2ull * dim * dim;
+  for (int i = 0; i < b; ++i) reqs[i] = Req{fn, tier, dim, m + i * stride};
+  std::lock_guard<std::mutex> lk(s->mu);
+  RunOpts opt;
+  return run_batch(s, reqs, o, aux, st, opt);
+}
+
+// Status -> value convention of the reference: off-domain / uncertifiable -> NaN.
+static void apply_status(int b, double* o, const int* st) {
+  for (int i = 0; i < b; ++i)
+    if (st[i] != kStOk) { o[2 * i] = NAN; o[2 * i + 1] = NAN; }
+}
+
+static int one_shot(int fn, int tier, const double* m, int dim, int b, double* o, double* aux) {
+  gbs_session* s;
+  int rc = with_default(&s);
+  if (rc) return rc;
+  std::vector<int> st(std::max(b, 0));
+  rc = uniform(s, fn, tier, m, dim, b, o, aux, st.data());
+  if (rc == 0) apply_status(b, o, st.data());
+  return rc;
+}
+
+// auto tier: fp64 + indicator, then the elements with kappa >= threshold rerun in
+// double-double on the device.  tier_out: 0 = fp64 kept, 1 = dd rerun.
+static int auto_batch(gbs_session* s, const std::vector<Req>& reqs, double kappa_max, double* out, double* kappa,
+                      int* tier_out, int* st) {
+  const int B = (int)reqs.size();
+  std::vector<Req> kreq = reqs;
+  for (Req& r : kreq) r.tier = kTierKappa;
+  std::vector<double> absn(B);
+  RunOpts opt;
+  int rc = run_batch(s, kreq, out, absn.data(), st, opt);
+  if (rc) return rc;
+  std::vector<Req> rerun;
+  std::vector<int> idx;
+  for (int i = 0; i < B; ++i) {
+    const double mag = std::max(std::hypot(out[2 * i], out[2 * i + 1]), 1e-300);
+    const double k = absn[i] / mag;
+    if (kappa) kappa[i] = k;
+    tier_out[i] = 0;
+    if (st[i] == kStOk && !(k < kappa_max)) {
+      Req r = reqs[i];
+      r.tier = kTierDD;
+      rerun.push_back(r);
+      idx.push_back(i);
+    }
+  }
+  if (!rerun.empty()) {
+    std::vector<double> o2(2 * rerun.size());
+    std::vector<int> s2(rerun.size());
+    rc = run_batch(s, rerun, o2.data(), nullptr, s2.data(), opt);
+    if (rc) return rc;
+    for (size_t j = 0; j < idx.size(); ++j) {
+      out[2 * idx[j]] = o2[2 * j];
+      out[2 * idx[j] + 1] = o2[2 * j + 1];
+      st[idx[j]] = s2[j];
+      tier_out[idx[j]] = 1;
+    }
+  }
+  return 0;
+}
+
+}  // namespace gbsb
+
+// ====================================================================== C ABI
+using namespace gbsb;
+
+extern "C" {
+
+const char* gbs_last_error(void) { return g_last_error.c_str(); }
+
+int gbs_version(void) { return 100; }
+
+// ---- one-shot uniform batches (core/host_api.cu:150-268) --------------------
+int gbs_perm_host(const double* m, int n, int b, double* o) { return one_shot(kFnPerm, kTierFp64, m, n, b, o, nullptr); }
+int gbs_perm_dd_host(const double* m, int n, int b, double* o) { return one_shot(kFnPerm, kTierDD, m, n, b, o, nullptr); }
+int gbs_haf_host(const double* m, int N, int b, double* o) { return one_shot(kFnHaf, kTierFp64, m, N, b, o, nullptr); }
+int gbs_haf_dd_host(const double* m, int N, int b, double* o) { return one_shot(kFnHaf, kTierDD, m, N, b, o, nullptr); }
+int gbs_lhaf_host(const double* m, int N, int b, double* o) { return one_shot(kFnLhaf, kTierFp64, m, N, b, o, nullptr); }
+int gbs_lhaf_dd_host(const double* m, int N, int b, double* o) { return one_shot(kFnLhaf, kTierDD, m, N, b, o, nullptr); }
+int gbs_tor_host(const double* m, int n, int b, double* o) { return one_shot(kFnTor, kTierFp64, m, 2 * n, b, o, nullptr); }
+int gbs_tor_dd_host(const double* m, int n, int b, double* o) { return one_shot(kFnTor, kTierDD, m, 2 * n, b, o, nullptr); }
+
+int gbs_perm_kappa_host(const double* m, int n, int b, double* o, double* a) { return one_shot(kFnPerm, kTierKappa, m, n, b, o, a); }
+int gbs_haf_kappa_host(const double* m, int N, int b, double* o, double* a) { return one_shot(kFnHaf, kTierKappa, m, N, b, o, a); }
+int gbs_lhaf_kappa_host(const double* m, int N, int b, double* o, double* a) { return one_shot(kFnLhaf, kTierKappa, m, N, b, o, a); }
+int gbs_tor_kappa_host(const double* m, int n, int b, double* o, double* a) { return one_shot(kFnTor, kTierKappa, m, 2 * n, b, o, a); }
+
+// ---- auto tier on the device (gbskernels/__init__.py:272-297) ----------------
+// func: 0 perm, 1 haf, 2 lhaf, 3 tor; dim = matrix side.  tier_out: 0 fp64, 1 dd.
+int gbs_auto_host(int func, const double* m, int dim, int b, double kappa_max, double* o, double* kappa,
+                  int* tier_out) {
+  if (b <= 0) return 0;
+  if (!m || !o || !tier_out) return fail(cudaErrorInvalidValue, "null buffer");
+  gbs_session* s;
+  int rc = with_default(&s);
+  if (rc) return rc;
+  std::vector<Req> reqs(b);
+  const size_t stride = 2ull * dim * dim;
+  for (int i = 0; i < b; ++i) reqs[i] = Req{func, kTierFp64, dim, m + i * stride};
+  std::vector<int> st(b);
+  std::lock_guard<std::mutex> lk(s->mu);
+  rc = auto_batch(s, reqs, kappa_max, o, kappa, tier_out, st.data());
+  if (rc == 0) apply_status(b, o, st.data());
+  return rc;
+}
+
+// ---- sessions (core/host_api.cu:521-658) --------------------------------------
+int gbs_session_open(gbs_session** out) {
+  if (!out) return fail(cudaErrorInvalidValue, "null session pointer");
+  return session_open(out);
+}
+int gbs_session_close(gbs_session* s) {
+  session_free(s);
+  return 0;
+}
+size_t gbs_session_reallocs(const gbs_session* s) { return s ? s->reallocs : 0; }
+
+// func: 0 perm, 1 haf, 2 lhaf, 3 tor; prec: 0 fp64, 1 dd, 2 fp64 + sum|term| (aux).
+int gbs_session_evaluate(gbs_session* s, int func, int prec, const double* h_mats, int dim, int batch,
+                         double* h_out) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  if (batch <= 0) return 0;
+  std::vector<int> st(batch);
+  int rc = uniform(s, func, prec, h_mats, dim, batch, h_out, nullptr, st.data());
+  if (rc == 0) apply_status(batch, h_out, st.data());
+  return rc;
+}
+
+// Device-resident output: evaluate, then copy the (B,) complex results into a fresh
+// device buffer owned by the caller (freed by gbs_dev_free).
+int gbs_session_evaluate_resident(gbs_session* s, int func, int prec, const double* h_mats, int dim, int batch,
+                                  double** d_result) {
+  if (!s || !d_result) return fail(cudaErrorInvalidValue, "null argument");
+  *d_result = nullptr;
+  if (batch <= 0) return 0;
+  std::vector<double> h(2 * (size_t)batch);
+  std::vector<int> st(batch);
+  int rc = uniform(s, func, prec, h_mats, dim, batch, h.data(), nullptr, st.data());
+  if (rc) return rc;
+  apply_status(batch, h.data(), st.data());
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, h.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (d) cudaFree(d);
+    return fail(e, "resident output");
+  }
+  *d_result = d;
+  return 0;
+}
+int gbs_dev_to_host(const double* d, double* h, int n) {
+  if (n <= 0) return 0;
+  return (int)cudaMemcpy(h, d, (size_t)n * 2 * sizeof(double), cudaMemcpyDeviceToHost);
+}
+int gbs_dev_free(double* d) {
+  cudaFree(d);
+  return 0;
+}
+
+// ---- ragged / mixed batches ----------------------------------------------------
+// B requests: funcs[i], tiers[i] (0 fp64, 1 dd, 2 fp64 + sum|term|), dims[i] (matrix
+// side), offsets[i] (in complex elements) into the packed host buffer `mats`.
+// mode: 0 = persistent mixed queue (one launch), 1 = plain per-size launches.
+int gbs_queue_evaluate(gbs_session* s, int B, const int* funcs, const int* tiers, const int* dims,
+                       const long long* offsets, const double* mats, int mode, double* out, double* aux,
+                       int* status) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  if (B <= 0) return 0;
+  if (!funcs || !tiers || !dims || !offsets || !mats || !out) return fail(cudaErrorInvalidValue, "null buffer");
+  std::vector<Req> reqs(B);
+  for (int i = 0; i < B; ++i) reqs[i] = Req{funcs[i], tiers[i], dims[i], mats + 2 * offsets[i]};
+  std::vector<int> st(B);
+  RunOpts opt;
+  opt.per_size = (mode == 1);
+  std::lock_guard<std::mutex> lk(s->mu);
+  int rc = run_batch(s, reqs, out, aux, st.data(), opt);
+  if (rc) return rc;
+  if (status) std::memcpy(status, st.data(), sizeof(int) * B);
+  apply_status(B, out, st.data());
+  return 0;
+}
+
+// Launch statistics of the session's last evaluation.
+int gbs_session_last_stats(const gbs_session* s, double* kernel_ms, int* launches, long long* items) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  if (kernel_ms) *kernel_ms = s->last_kernel_ms;
+  if (launches) *launches = s->last_launches;
+  if (items) *items = s->last_items;
+  return 0;
+}
+
+}  // extern "C"
