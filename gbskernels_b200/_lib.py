@@ -54,6 +54,10 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_queue_evaluate": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int, _dp, _dp, _ip],
                            ctypes.c_int),
     "gbs_session_last_stats": ([_vp, _dp, _ip, _llp], ctypes.c_int),
+    "gbs_queue_prepare": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int], ctypes.c_int),
+    "gbs_queue_run": ([_vp, _vp], ctypes.c_int),
+    "gbs_queue_read": ([_vp, _vp, _dp, _dp, _ip], ctypes.c_int),
+    "gbs_probe_fp64_peak": ([_dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
 }
 
 _LIB = None

@@ -145,7 +145,8 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
   } else if (fn == kFnHaf || fn == kFnLhaf) {
     const int n = dim_eval / 2;
     const unsigned long long masks = 1ull << n;
-    const int per = tier == kTierDD ? std::max(0, n - 9) : std::max(0, n - 7);
+    // masks per item: 2^9 (binary64) / 2^6 (double-double); smaller instances are one item
+    const int per = tier == kTierDD ? std::min(n, 6) : std::min(n, 9);
     const unsigned long long cnt = 1ull << per;
     for (unsigned long long lo = 0; lo < masks; lo += cnt) add(lo, std::min(cnt, masks - lo));
     P.haf_smax = std::max(P.haf_smax, dim_eval);
@@ -199,6 +200,21 @@ struct gbs_session {
   float last_kernel_ms = 0.f;
   int last_launches = 0;
   long long last_items = 0;
+  // the current plan (device-resident work queue of the last prepared batch)
+  struct Group {
+    gbsb::ItemLaunch L;
+    unsigned br = 0;
+    int grid = 0, warps = 0;
+    int ni = 0, nit = 0;
+    size_t out_off = 0;     // instance offset into the session's result arrays
+    std::vector<int> req;   // request index of each instance
+  };
+  std::vector<Group> groups;
+  int plan_B = 0;
+  std::vector<char> plan_trivial;
+  std::vector<gbsb::cplx> plan_tval;
+  size_t plan_ninst = 0;
+  bool plan_ready = false;
   std::mutex mu;
 };
 
@@ -285,86 +301,74 @@ struct RunOpts {
   int warps = 4;           // warps per block
 };
 
-// Core: evaluate `reqs` on the session stream.  out: 2 doubles per request, aux: 1
-// double per request (sum |term|, kappa tier), st: status per request.
-static int run_batch(gbs_session* s, const std::vector<Req>& reqs, double* out, double* aux, int* st,
-                     const RunOpts& opt) {
+// Build the device-resident plan of `reqs`: validate, pack and upload every matrix
+// once, cut the work items, upload the queue(s).  One group = one launch: a single
+// group holds every haf / lhaf / tor request (persistent mixed queue); the
+// permanent gets one group per tier; per-size mode gives one group per
+// (func, tier, size) bucket.
+static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpts& opt) {
+  s->plan_ready = false;
+  s->groups.clear();
   const int B = (int)reqs.size();
-  if (B == 0) return 0;
-  // ---- validate & size
+  s->plan_B = B;
+  s->plan_trivial.assign(B, 0);
+  s->plan_tval.assign(B, mkc(0, 0));
+  s->plan_ninst = 0;
+  if (B == 0) { s->plan_ready = true; return 0; }
   std::vector<int> dim_eval(B, 0);
-  std::vector<char> real_in(B, 0), trivial(B, 0);
-  std::vector<cplx> tval(B);
+  std::vector<char> real_in(B, 0);
   long long mat_doubles = 0;
   for (int i = 0; i < B; ++i) {
     bool re = false, tr = false;
-    int rc = check_req(reqs[i], &dim_eval[i], &re, &tr, &tval[i]);
+    int rc = check_req(reqs[i], &dim_eval[i], &re, &tr, &s->plan_tval[i]);
     if (rc) {
       g_last_error = "request #" + std::to_string(i) + ": " + g_last_error;
       return rc;
     }
     real_in[i] = re;
-    trivial[i] = tr;
+    s->plan_trivial[i] = tr;
     if (!tr) mat_doubles += 2ll * dim_eval[i] * dim_eval[i];
   }
-  // ---- group (per-size) or single queue
   std::vector<std::vector<int>> groups;
   if (opt.per_size) {
     std::vector<long long> keys;
     for (int i = 0; i < B; ++i) {
-      if (trivial[i]) continue;
+      if (s->plan_trivial[i]) continue;
       long long key = ((long long)reqs[i].fn * 8 + reqs[i].tier) * 4096 + dim_eval[i];
       size_t g = std::find(keys.begin(), keys.end(), key) - keys.begin();
       if (g == keys.size()) { keys.push_back(key); groups.emplace_back(); }
       groups[g].push_back(i);
     }
   } else {
-    // one persistent launch for every haf / lhaf / tor request; the permanent runs
-    // its own queue (one per tier) because its register budget differs
     groups.resize(4);
     for (int i = 0; i < B; ++i) {
-      if (trivial[i]) continue;
+      if (s->plan_trivial[i]) continue;
       groups[reqs[i].fn == kFnPerm ? 1 + reqs[i].tier : 0].push_back(i);
     }
   }
-  // ---- upload every matrix once (pinned staging, one H2D)
-  cudaError_t e = grow_pin(s->pin_in, std::max<long long>(mat_doubles, 2) * sizeof(double));
-  if (e == cudaSuccess) e = grow_dev(s->mats, std::max<long long>(mat_doubles, 2) * sizeof(double), &s->reallocs);
-  if (e != cudaSuccess) return fail(e, "allocating matrix buffers");
+  // ---- plans of every group (host) and the sizes of the concatenated device arrays
+  std::vector<Plan> plans;
+  std::vector<std::vector<int>> greq;
+  for (auto& grp : groups) {
+    if (grp.empty()) continue;
+    plans.emplace_back();
+    greq.push_back(grp);
+  }
   std::vector<long long> off(B, 0);
   {
-    double* dst = (double*)s->pin_in.p;
     long long o = 0;
     for (int i = 0; i < B; ++i) {
-      if (trivial[i]) continue;
+      if (s->plan_trivial[i]) continue;
       off[i] = o;
-      const int d = reqs[i].dim, de = dim_eval[i];
-      if (de == d) {
-        std::memcpy(dst + o, reqs[i].mat, sizeof(double) * 2 * (size_t)d * d);
-      } else {  // odd loop hafnian: A (+) [1]
-        std::memset(dst + o, 0, sizeof(double) * 2 * (size_t)de * de);
-        for (int r = 0; r < d; ++r)
-          std::memcpy(dst + o + 2ll * r * de, reqs[i].mat + 2ll * r * d, sizeof(double) * 2 * d);
-        dst[o + 2ll * ((long long)d * de + d)] = 1.0;
-      }
-      o += 2ll * de * de;
+      o += 2ll * dim_eval[i] * dim_eval[i];
     }
   }
-  if (mat_doubles > 0) {
-    e = cudaMemcpyAsync(s->mats.p, s->pin_in.p, mat_doubles * sizeof(double), cudaMemcpyHostToDevice, s->stream);
-    if (e != cudaSuccess) return fail(e, "uploading matrices");
-  }
-  s->last_launches = 0;
-  s->last_items = 0;
-  float kernel_ms = 0.f;
-  // ---- one launch per group
-  for (const std::vector<int>& grp : groups) {
-    if (grp.empty()) continue;
-    Plan P;
-    for (int i : grp) plan_instance(P, reqs[i].fn, reqs[i].tier, dim_eval[i], real_in[i], off[i]);
+  size_t meta_bytes = 0, tot_items = 0, tot_inst = 0;
+  for (size_t g = 0; g < plans.size(); ++g) {
+    Plan& P = plans[g];
+    for (int i : greq[g]) plan_instance(P, reqs[i].fn, reqs[i].tier, dim_eval[i], real_in[i], off[i]);
     P.ws_doubles = ws_for_plan(P);
     const int ni = (int)P.insts.size(), nit = (int)P.items.size();
-    // queue order: instances heaviest first (items of one instance stay contiguous)
     std::vector<int> inst_order(ni);
     for (int k = 0; k < ni; ++k) inst_order[k] = k;
     if (opt.sort_heavy && !opt.per_size) {
@@ -378,91 +382,173 @@ static int run_batch(gbs_session* s, const std::vector<Req>& reqs, double* out, 
     P.order.reserve(nit);
     for (int k : inst_order)
       for (int j = 0; j < P.insts[k].nitems; ++j) P.order.push_back(P.insts[k].item0 + j);
-    unsigned br = cover(P.need);
-    if (br == 0) return fail(cudaErrorNotSupported, "batch mixes the permanent with other functions");
-    // ---- buffers
-    const size_t meta_bytes = ni * sizeof(InstDesc) + nit * sizeof(WorkItem) + nit * sizeof(int);
-    e = grow_pin(s->pin_meta, meta_bytes);
-    if (e == cudaSuccess) e = grow_dev(s->meta, meta_bytes, &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->part, (size_t)nit * 4 * sizeof(double), &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->paux, (size_t)nit * sizeof(double), &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->pst, (size_t)nit * sizeof(int), &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->done, (size_t)ni * sizeof(int), &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->head, 16, &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->out, (size_t)ni * 2 * sizeof(double), &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->aux, (size_t)ni * sizeof(double), &s->reallocs);
-    if (e == cudaSuccess) e = grow_dev(s->st, (size_t)ni * sizeof(int), &s->reallocs);
-    if (e == cudaSuccess) e = grow_pin(s->pin_out, (size_t)ni * (3 * sizeof(double) + sizeof(int)));
-    if (e != cudaSuccess) return fail(e, "allocating work buffers");
-    // the meta upload must not overwrite staging still in flight from a previous group
-    e = cudaStreamSynchronize(s->stream);
-    if (e != cudaSuccess) return fail(e, "synchronising before upload");
-    char* pm = (char*)s->pin_meta.p;
-    std::memcpy(pm, P.insts.data(), ni * sizeof(InstDesc));
-    std::memcpy(pm + ni * sizeof(InstDesc), P.items.data(), nit * sizeof(WorkItem));
-    std::memcpy(pm + ni * sizeof(InstDesc) + nit * sizeof(WorkItem), P.order.data(), nit * sizeof(int));
-    e = cudaMemcpyAsync(s->meta.p, pm, meta_bytes, cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->head.p, 0, 16, s->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->done.p, 0, (size_t)ni * sizeof(int), s->stream);
-    if (e != cudaSuccess) return fail(e, "uploading the work queue");
-    ItemLaunch L{};
+    if (cover(P.need) == 0) return fail(cudaErrorNotSupported, "no compiled kernel covers this mix");
+    meta_bytes += ((ni * sizeof(InstDesc) + nit * sizeof(WorkItem) + nit * sizeof(int)) + 255) & ~(size_t)255;
+    tot_items += nit;
+    tot_inst += ni;
+  }
+  // ---- buffers (monotone growth)
+  cudaError_t e = grow_pin(s->pin_in, std::max<long long>(mat_doubles, 2) * sizeof(double));
+  if (e == cudaSuccess) e = grow_dev(s->mats, std::max<long long>(mat_doubles, 2) * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_pin(s->pin_meta, std::max<size_t>(meta_bytes, 256));
+  if (e == cudaSuccess) e = grow_dev(s->meta, std::max<size_t>(meta_bytes, 256), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->part, std::max<size_t>(tot_items, 1) * 4 * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->paux, std::max<size_t>(tot_items, 1) * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->pst, std::max<size_t>(tot_items, 1) * sizeof(int), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->done, std::max<size_t>(tot_inst, 1) * sizeof(int), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->head, 64 * std::max<size_t>(plans.size(), 1), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->out, std::max<size_t>(tot_inst, 1) * 2 * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->aux, std::max<size_t>(tot_inst, 1) * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->st, std::max<size_t>(tot_inst, 1) * sizeof(int), &s->reallocs);
+  if (e == cudaSuccess) e = grow_pin(s->pin_out, std::max<size_t>(tot_inst, 1) * (3 * sizeof(double) + sizeof(int)));
+  if (e != cudaSuccess) return fail(e, "allocating session buffers");
+  // staging buffers may still be read by copies of a previous call
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return fail(e, "synchronising the session stream");
+  // ---- pack matrices (odd loop hafnians augmented by A (+) [1]) and upload once
+  {
+    double* dst = (double*)s->pin_in.p;
+    for (int i = 0; i < B; ++i) {
+      if (s->plan_trivial[i]) continue;
+      const long long o = off[i];
+      const int d = reqs[i].dim, de = dim_eval[i];
+      if (de == d) {
+        std::memcpy(dst + o, reqs[i].mat, sizeof(double) * 2 * (size_t)d * d);
+      } else {
+        std::memset(dst + o, 0, sizeof(double) * 2 * (size_t)de * de);
+        for (int r = 0; r < d; ++r)
+          std::memcpy(dst + o + 2ll * r * de, reqs[i].mat + 2ll * r * d, sizeof(double) * 2 * d);
+        dst[o + 2ll * ((long long)d * de + d)] = 1.0;
+      }
+    }
+    if (mat_doubles > 0) {
+      e = cudaMemcpyAsync(s->mats.p, s->pin_in.p, mat_doubles * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+      if (e != cudaSuccess) return fail(e, "uploading matrices");
+    }
+  }
+  // ---- queues
+  size_t moff = 0, ioff = 0, noff = 0;
+  char* pm = (char*)s->pin_meta.p;
+  for (size_t g = 0; g < plans.size(); ++g) {
+    Plan& P = plans[g];
+    const int ni = (int)P.insts.size(), nit = (int)P.items.size();
+    // shift item0 of every instance and the order entries to this group's slots
+    std::memcpy(pm + moff, P.insts.data(), ni * sizeof(InstDesc));
+    std::memcpy(pm + moff + ni * sizeof(InstDesc), P.items.data(), nit * sizeof(WorkItem));
+    std::memcpy(pm + moff + ni * sizeof(InstDesc) + nit * sizeof(WorkItem), P.order.data(), nit * sizeof(int));
+    gbs_session::Group G;
+    ItemLaunch& L = G.L;
+    char* dm = (char*)s->meta.p + moff;
     L.mats = (const double*)s->mats.p;
-    L.insts = (const InstDesc*)s->meta.p;
-    L.items = (const WorkItem*)((char*)s->meta.p + ni * sizeof(InstDesc));
-    L.order = (const int*)((char*)s->meta.p + ni * sizeof(InstDesc) + nit * sizeof(WorkItem));
+    L.insts = (const InstDesc*)dm;
+    L.items = (const WorkItem*)(dm + ni * sizeof(InstDesc));
+    L.order = (const int*)(dm + ni * sizeof(InstDesc) + nit * sizeof(WorkItem));
     L.n_items = nit;
-    L.head = (int*)s->head.p;
-    L.done = (int*)s->done.p;
-    L.part = (double*)s->part.p;
-    L.paux = (double*)s->paux.p;
-    L.pst = (int*)s->pst.p;
-    L.out = (double*)s->out.p;
-    L.aux_out = (double*)s->aux.p;
-    L.st_out = (int*)s->st.p;
+    L.head = (int*)((char*)s->head.p + 64 * g);
+    L.done = (int*)s->done.p + noff;
+    L.part = (double*)s->part.p + 4 * ioff;
+    L.paux = (double*)s->paux.p + ioff;
+    L.pst = (int*)s->pst.p + ioff;
+    L.out = (double*)s->out.p + 2 * noff;
+    L.aux_out = (double*)s->aux.p + noff;
+    L.st_out = (int*)s->st.p + noff;
     L.ws_doubles = P.ws_doubles;
     L.haf_smax = P.haf_smax;
+    G.br = cover(P.need);
     int warps = opt.warps;
     const size_t smem_per_warp = (size_t)P.ws_doubles * sizeof(double);
     while (warps > 1 && (size_t)warps * smem_per_warp > 200 * 1024) warps >>= 1;
-    int bps = occ_any(br, L, warps);
+    const int bps = occ_any(G.br, L, warps);
     if (bps <= 0) return fail(cudaErrorInvalidConfiguration, "work item kernel does not fit on an SM");
-    long long want_blocks = (nit + warps - 1) / warps;
-    int grid = (int)std::min<long long>((long long)s->sms * bps, want_blocks);
-    cudaEventRecord(s->ev0, s->stream);
-    e = launch_any(br, L, grid, warps, s->stream);
-    cudaEventRecord(s->ev1, s->stream);
-    if (e != cudaSuccess) return fail(e, "launching the work item kernel");
-    // ---- results
-    double* po = (double*)s->pin_out.p;
-    double* pa = po + 2 * ni;
-    int* ps = (int*)(pa + ni);
-    e = cudaMemcpyAsync(po, s->out.p, (size_t)ni * 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(pa, s->aux.p, (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ps, s->st.p, (size_t)ni * sizeof(int), cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    if (e != cudaSuccess) return fail(e, "evaluating the batch");
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-    kernel_ms += ms;
-    s->last_launches += 1;
-    s->last_items += nit;
-    for (int k = 0; k < ni; ++k) {
-      const int i = grp[k];
-      out[2 * i] = po[2 * k];
-      out[2 * i + 1] = po[2 * k + 1];
-      if (aux) aux[i] = pa[k];
-      if (st) st[i] = ps[k];
-    }
+    const long long want_blocks = (nit + warps - 1) / warps;
+    G.grid = (int)std::min<long long>((long long)s->sms * bps, want_blocks);
+    G.warps = warps;
+    G.ni = ni;
+    G.nit = nit;
+    G.out_off = noff;
+    G.req = greq[g];
+    s->groups.push_back(std::move(G));
+    moff += ((ni * sizeof(InstDesc) + nit * sizeof(WorkItem) + nit * sizeof(int)) + 255) & ~(size_t)255;
+    ioff += nit;
+    noff += ni;
   }
-  s->last_kernel_ms = kernel_ms;
-  for (int i = 0; i < B; ++i) {
-    if (!trivial[i]) continue;
-    out[2 * i] = tval[i].re;
-    out[2 * i + 1] = tval[i].im;
-    if (aux) aux[i] = std::hypot(tval[i].re, tval[i].im);
+  if (moff > 0) {
+    e = cudaMemcpyAsync(s->meta.p, pm, moff, cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return fail(e, "uploading the work queues");
+  }
+  s->plan_ninst = noff;
+  s->plan_ready = true;
+  return 0;
+}
+
+// Launch the prepared plan on `stream` (the session stream when null): reset the
+// queue heads and completion counters, then one kernel per group.
+static int plan_launch(gbs_session* s, cudaStream_t stream) {
+  if (!s->plan_ready) return fail(cudaErrorInvalidValue, "no prepared plan");
+  if (!stream) stream = s->stream;
+  cudaError_t e = cudaSuccess;
+  if (!s->groups.empty()) {
+    e = cudaMemsetAsync(s->head.p, 0, 64 * s->groups.size(), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->done.p, 0, s->plan_ninst * sizeof(int), stream);
+  }
+  if (e != cudaSuccess) return fail(e, "resetting the work queues");
+  cudaEventRecord(s->ev0, stream);
+  long long items = 0;
+  for (auto& G : s->groups) {
+    e = launch_any(G.br, G.L, G.grid, G.warps, stream);
+    if (e != cudaSuccess) return fail(e, "launching the work item kernel");
+    items += G.nit;
+  }
+  cudaEventRecord(s->ev1, stream);
+  s->last_launches = (int)s->groups.size();
+  s->last_items = items;
+  return 0;
+}
+
+// Copy the plan's results back (synchronous) and scatter them to request order.
+static int plan_read(gbs_session* s, cudaStream_t stream, double* out, double* aux, int* st) {
+  if (!stream) stream = s->stream;
+  const size_t ni = s->plan_ninst;
+  double* po = (double*)s->pin_out.p;
+  double* pa = po + 2 * ni;
+  int* ps = (int*)(pa + ni);
+  cudaError_t e = cudaSuccess;
+  if (ni > 0) {
+    e = cudaMemcpyAsync(po, s->out.p, ni * 2 * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pa, s->aux.p, ni * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ps, s->st.p, ni * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(e, "evaluating the batch");
+  float ms = 0.f;
+  if (!s->groups.empty()) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  s->last_kernel_ms = ms;
+  for (const auto& G : s->groups)
+    for (int k = 0; k < G.ni; ++k) {
+      const int i = G.req[k];
+      out[2 * i] = po[2 * (G.out_off + k)];
+      out[2 * i + 1] = po[2 * (G.out_off + k) + 1];
+      if (aux) aux[i] = pa[G.out_off + k];
+      if (st) st[i] = ps[G.out_off + k];
+    }
+  for (int i = 0; i < s->plan_B; ++i) {
+    if (!s->plan_trivial[i]) continue;
+    const cplx t = s->plan_tval[i];
+    out[2 * i] = t.re;
+    out[2 * i + 1] = t.im;
+    if (aux) aux[i] = std::hypot(t.re, t.im);
     if (st) st[i] = kStOk;
   }
   return 0;
+}
+
+static int run_batch(gbs_session* s, const std::vector<Req>& reqs, double* out, double* aux, int* st,
+                     const RunOpts& opt) {
+  if (reqs.empty()) return 0;
+  int rc = plan_build(s, reqs, opt);
+  if (rc == 0) rc = plan_launch(s, nullptr);
+  if (rc == 0) rc = plan_read(s, nullptr, out, aux, st);
+  return rc;
 }
 
 // ------------------------------------------------------------------ process-wide default session
@@ -695,6 +781,42 @@ int gbs_queue_evaluate(gbs_session* s, int B, const int* funcs, const int* tiers
   if (rc) return rc;
   if (status) std::memcpy(status, st.data(), sizeof(int) * B);
   apply_status(B, out, st.data());
+  return 0;
+}
+
+// Device-resident plan: upload + cut once (gbs_queue_prepare), launch many times
+// (gbs_queue_run, on `stream` or the session stream when null), read back
+// (gbs_queue_read).  Inputs stay in HBM between runs.
+int gbs_queue_prepare(gbs_session* s, int B, const int* funcs, const int* tiers, const int* dims,
+                      const long long* offsets, const double* mats, int mode) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  if (B < 0 || (B > 0 && (!funcs || !tiers || !dims || !offsets || !mats)))
+    return fail(cudaErrorInvalidValue, "null buffer");
+  std::vector<Req> reqs(B);
+  for (int i = 0; i < B; ++i) reqs[i] = Req{funcs[i], tiers[i], dims[i], mats + 2 * offsets[i]};
+  RunOpts opt;
+  opt.per_size = (mode == 1);
+  std::lock_guard<std::mutex> lk(s->mu);
+  int rc = plan_build(s, reqs, opt);
+  if (rc == 0) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) rc = fail(e, "uploading the plan");
+  }
+  return rc;
+}
+int gbs_queue_run(gbs_session* s, void* stream) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  std::lock_guard<std::mutex> lk(s->mu);
+  return plan_launch(s, (cudaStream_t)stream);
+}
+int gbs_queue_read(gbs_session* s, void* stream, double* out, double* aux, int* status) {
+  if (!s || !out) return fail(cudaErrorInvalidValue, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::vector<int> st(std::max(s->plan_B, 1));
+  int rc = plan_read(s, (cudaStream_t)stream, out, aux, st.data());
+  if (rc) return rc;
+  if (status) std::memcpy(status, st.data(), sizeof(int) * s->plan_B);
+  apply_status(s->plan_B, out, st.data());
   return 0;
 }
 

@@ -1,0 +1,104 @@
+/* gbs_b200.h -- C ABI of libgbs_b200.so: batched permanents, hafnians, loop
+ * hafnians and torontonians on NVIDIA B200 (sm_100a).
+ *
+ * Drop-in for the reference's host API (chaofanzhougit/GBSKernels core/host_api.cu)
+ * and the entry points its Python binding calls (bindings/gbskernels_ext.cpp).
+ *
+ * Conventions (identical to the reference):
+ *   - complex matrices are interleaved (re, im) binary64 pairs, row-major, batch
+ *     contiguous: the memory of a numpy complex128 (B, d, d) array (the reference
+ *     types these pointers cuDoubleComplex*, which has the same layout);
+ *   - `n` is the matrix side for perm, the MODE count for tor (matrices 2n x 2n),
+ *     `N` the matrix side for haf / lhaf;
+ *   - every function returns 0 on success or a nonzero code (a cudaError_t value
+ *     or cudaErrorInvalidValue = 1 for bad arguments); gbs_last_error() describes
+ *     the last failure of the calling thread;
+ *   - the caller owns host buffers; the library owns device and pinned buffers.
+ *   - a torontonian off the physical domain (I - O_S not positive definite) or an
+ *     uncertifiable element yields NaN values (and +inf bounds), never an error.
+ */
+#ifndef GBS_B200_H
+#define GBS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gbs_session gbs_session;
+
+int gbs_version(void);
+const char* gbs_last_error(void);
+
+/* ---- one-shot uniform batches: H2D -> launch -> D2H ------------------------
+ * reference: core/host_api.cu:153-230 (gbs_perm_host ... gbs_tor_dd_host)     */
+int gbs_perm_host(const double* mats, int n, int batch, double* out);
+int gbs_perm_dd_host(const double* mats, int n, int batch, double* out);
+int gbs_haf_host(const double* mats, int N, int batch, double* out);
+int gbs_haf_dd_host(const double* mats, int N, int batch, double* out);
+/* odd N is evaluated as lhaf(A (+) [1]) (gbskernels/__init__.py:190-200) */
+int gbs_lhaf_host(const double* mats, int N, int batch, double* out);
+int gbs_lhaf_dd_host(const double* mats, int N, int batch, double* out);
+int gbs_tor_host(const double* mats, int n, int batch, double* out);
+int gbs_tor_dd_host(const double* mats, int n, int batch, double* out);
+
+/* ---- fp64 value + sum|term| (precision="auto" indicator) -------------------
+ * reference: core/host_api.cu:235-246 (gbs_*_kappa_host)                       */
+int gbs_perm_kappa_host(const double* mats, int n, int batch, double* out, double* absnorm);
+int gbs_haf_kappa_host(const double* mats, int N, int batch, double* out, double* absnorm);
+int gbs_lhaf_kappa_host(const double* mats, int N, int batch, double* out, double* absnorm);
+int gbs_tor_kappa_host(const double* mats, int n, int batch, double* out, double* absnorm);
+
+/* ---- auto tier on the device ----------------------------------------------
+ * reference: gbskernels/__init__.py:272-297 (_gpu_auto_batched) whose fp64 pass is
+ * gbs_*_kappa_host and whose rerun is gbs_*_dd_host; here both run in the library.
+ * func: 0 perm, 1 haf, 2 lhaf, 3 tor.  dim = matrix side (tor: 2n).  Elements
+ * with kappa = absnorm/|value| >= kappa_max are re-evaluated in double-double.
+ * tier_out[i]: 0 = fp64 value kept, 1 = double-double rerun.                    */
+int gbs_auto_host(int func, const double* mats, int dim, int batch, double kappa_max, double* out,
+                  double* kappa, int* tier_out);
+
+/* ---- resident sessions -------------------------------------------------------
+ * reference: core/host_api.cu:521-658 (gbs_session_open ... gbs_dev_free)
+ * func: 0 perm, 1 haf, 2 lhaf, 3 tor; prec: 0 fp64, 1 dd.  dim = matrix side.  */
+int gbs_session_open(gbs_session** out);
+int gbs_session_close(gbs_session* s);
+size_t gbs_session_reallocs(const gbs_session* s);
+int gbs_session_evaluate(gbs_session* s, int func, int prec, const double* mats, int dim, int batch,
+                         double* out);
+int gbs_session_evaluate_resident(gbs_session* s, int func, int prec, const double* mats, int dim,
+                                  int batch, double** d_result);
+int gbs_dev_to_host(const double* d_result, double* h_out, int n);
+int gbs_dev_free(double* d_result);
+
+/* ---- ragged, mixed-function, mixed-tier batches ----------------------------
+ * reference: gbskernels/__init__.py:813-852 (Workspace._ragged: one launch per
+ * size bucket).  mode 0: ONE persistent launch over a device work queue holding
+ * every instance (functions, sizes and tiers mixed); mode 1: one launch per
+ * (function, tier, size) bucket.  offsets[i] is in complex elements into `mats`.
+ * tiers[i]: 0 fp64, 1 dd, 2 fp64 + sum|term| (aux[i]).  status[i]: 0 ok,
+ * 1 torontonian off the physical domain.                                         */
+int gbs_queue_evaluate(gbs_session* s, int batch, const int* funcs, const int* tiers, const int* dims,
+                       const long long* offsets, const double* mats, int mode, double* out, double* aux,
+                       int* status);
+/* device-resident plan: validate, cut and upload once; run many times on `stream`
+ * (a cudaStream_t, or NULL for the session stream); read results back.  Used for
+ * timing with inputs resident in HBM and by servers that re-run a fixed batch.   */
+int gbs_queue_prepare(gbs_session* s, int batch, const int* funcs, const int* tiers, const int* dims,
+                      const long long* offsets, const double* mats, int mode);
+int gbs_queue_run(gbs_session* s, void* stream);
+int gbs_queue_read(gbs_session* s, void* stream, double* out, double* aux, int* status);
+/* kernel time (CUDA events), launches and work items of the session's last call */
+int gbs_session_last_stats(const gbs_session* s, double* kernel_ms, int* launches, long long* items);
+
+/* ---- measurement ------------------------------------------------------------
+ * FP64 tensor-core throughput of this GPU (mma .m16n8k8 .f64 chains on every SM),
+ * the denominator of the kernels' roofline fraction.  No reference counterpart.  */
+int gbs_probe_fp64_peak(double* tflops, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GBS_B200_H */

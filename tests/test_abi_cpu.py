@@ -1,0 +1,110 @@
+"""The C-ABI surface and the host-side argument checks (CPU only, no device calls)."""
+
+from __future__ import annotations
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_symbols() -> list[str]:
+    names = []
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"\b(gbs_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_header_declares_the_reference_host_api():
+    names = set(_declared_symbols())
+    # the reference's core/host_api.cu entry points for this path
+    for f in ("perm", "perm_dd", "haf", "haf_dd", "lhaf", "lhaf_dd", "tor", "tor_dd"):
+        assert f"gbs_{f}_host" in names
+    for f in ("perm", "haf", "lhaf", "tor"):
+        assert f"gbs_{f}_kappa_host" in names
+    for f in ("open", "evaluate", "evaluate_resident", "close", "reallocs"):
+        assert f"gbs_session_{f}" in names
+    assert {"gbs_dev_to_host", "gbs_dev_free", "gbs_queue_evaluate"} <= names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in _declared_symbols() if not hasattr(lib, n)]
+    assert not missing, f"libgbs_b200.so lacks {missing}"
+
+
+def test_binding_covers_every_declared_symbol():
+    from gbskernels_b200 import _lib
+    missing = [n for n in _declared_symbols() if n not in _lib.SIGNATURES]
+    assert not missing
+
+
+def test_library_is_sm100a(lib):
+    from gbskernels_b200 import build
+    assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
+    assert lib.gbs_version() >= 100
+
+
+# ---- argument checks that fail before any device work (reference semantics) ----
+def test_precision_and_backend_errors(G):
+    A = np.eye(4)
+    with pytest.raises(ValueError, match="unknown backend"):
+        G.haf(A, backend="tpu")
+    with pytest.raises(NotImplementedError):
+        G.haf(A, backend="cpu")
+    with pytest.raises(NotImplementedError, match="CPU only"):
+        G.haf(A, precision="ref")
+    with pytest.raises(ValueError, match="unknown precision"):
+        G.haf(A, precision="fp32")
+    with pytest.raises(ValueError, match="return_diagnostics"):
+        G.haf(A, precision="certified")
+    with pytest.raises(ValueError, match="requires precision='auto' or 'certified'"):
+        G.haf(A, return_diagnostics=True)
+    with pytest.raises(ValueError, match="rtol"):
+        G.haf(A, rtol=1e-3)
+    with pytest.raises(ValueError, match="rtol must be finite"):
+        G.haf(A, precision="certified", return_diagnostics=True, rtol=-1.0)
+
+
+def test_shape_and_cap_errors(G):
+    with pytest.raises(ValueError, match="uniform"):
+        G.haf_batched(np.zeros((2, 3, 4)))
+    with pytest.raises(ValueError, match="exceeds"):
+        G.perm_batched(np.zeros((1, 29, 29)))
+    with pytest.raises(ValueError, match="exceeds"):
+        G.haf_batched(np.zeros((1, 34, 34)))
+    with pytest.raises(ValueError, match="exceeds"):
+        G.lhaf_batched(np.zeros((1, 33, 33)))   # odd N augments to 34
+    with pytest.raises(ValueError, match="even"):
+        G.tor_batched(np.zeros((1, 3, 3)))
+    with pytest.raises(ValueError, match="real-domain"):
+        G.tor_batched(np.eye(4)[None] * (0.1 + 0.1j), precision="dd")
+    with pytest.raises(ValueError, match="finite"):
+        G.haf(np.full((2, 2), np.nan), precision="certified", return_diagnostics=True)
+
+
+def test_tor_single_contract_errors(G):
+    with pytest.raises(ValueError, match="even"):
+        G.tor_single(np.zeros((3, 3)))
+    with pytest.raises(ValueError, match="cap 64"):
+        G.tor_single(np.zeros((66, 66)))
+    with pytest.raises(ValueError, match="symmetric"):
+        O = np.zeros((4, 4)); O[0, 1] = 0.1
+        G.tor_single(O)
+    with pytest.raises(ValueError, match="real-domain"):
+        G.tor_single(np.eye(4) * 1j * 0.1)
+
+
+def test_workspace_lifecycle_errors(G):
+    ws = G.Workspace()
+    with pytest.raises(RuntimeError, match="entered"):
+        ws.haf_batched([np.eye(2)])
+    ws.close()
+    ws.close()  # idempotent
+    with pytest.raises(RuntimeError, match="closed"):
+        ws.haf_batched([np.eye(2)])
+    with pytest.raises(ValueError, match="unknown backend"):
+        G.Workspace(backend="tpu")

@@ -1,0 +1,276 @@
+"""Parity of the sm_100a kernels with the oracle and the reference's golden vectors.
+
+Tolerances: binary64 tiers must be within relative error 1e-10 of the ground truth
+(mpmath from the reference, or the binary128 oracle), the double-double tier within
+1e-15 (it is collapsed to binary64 at the API), and integer-valued closed forms are
+checked to 1e-12.  Reference test models: tests/test_layer1_combinatorial.py,
+tests/test_hafnian_layer1.py, tests/test_loop_hafnian.py, tests/test_torontonian.py,
+tests/test_layer5_engineering.py, tests/test_precision_auto.py.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+DD_TOL = 1e-15
+RNG = np.random.default_rng(123)
+
+
+def sym(N, cplx=True, scale=0.5):
+    X = RNG.standard_normal((N, N)) + (1j * RNG.standard_normal((N, N)) if cplx else 0)
+    return scale * (X + X.T) / 2
+
+
+def phys_O(n, scale=1.0):
+    X = RNG.standard_normal((2 * n, 2 * n))
+    S = scale * X @ X.T / (2 * n) + np.eye(2 * n)
+    O = np.eye(2 * n) - np.linalg.inv(S)
+    return (O + O.T) / 2
+
+
+def _batched(G, func):
+    return getattr(G, f"{func}_batched")
+
+
+# ---------------------------------------------------------------- golden vectors
+@pytest.mark.parametrize("func", ["perm", "haf", "lhaf", "tor"])
+@pytest.mark.parametrize("precision", ["fp64", "dd"])
+def test_golden_vectors(gpu, golden, func, precision):
+    for m, truth, _, i in golden_cases(golden, func):
+        if func == "tor" and np.any(np.imag(m) != 0):
+            continue  # complex O: not a batched-kernel input (the API rejects it)
+        v = _batched(gpu, func)(m[None], precision=precision)[0]
+        tol = FP64_TOL if precision == "fp64" else DD_TOL
+        if abs(truth) < 1e-6:
+            assert abs(v - truth) < 1e-13, (func, i)
+        else:
+            assert rel_err(v, truth) < tol, (func, precision, i, v, truth)
+
+
+@pytest.mark.parametrize("func", ["perm", "haf", "lhaf", "tor"])
+def test_golden_indicator(gpu, golden, func):
+    for m, truth, _, i in golden_cases(golden, func):
+        if func == "tor" and np.any(np.imag(m) != 0):
+            continue
+        if abs(truth) < 1e-6:
+            continue  # kappa is ill-defined at a zero value
+        v, diags = _batched(gpu, func)(m[None], precision="auto", return_diagnostics=True)
+        absn = golden[f"{func}_absnorm"][i]
+        kappa_ref = absn / max(abs(golden[f"{func}_cpu_fp64"][i]), 1e-300)
+        assert diags[0]["cancellation"] == pytest.approx(kappa_ref, rel=1e-6), (func, i)
+        assert diags[0]["tier"] in ("fp64", "dd")
+
+
+# ---------------------------------------------------------------- closed forms
+@pytest.mark.parametrize("n", [1, 2, 5, 8, 12, 16])
+def test_perm_closed_forms(gpu, n):
+    assert gpu.perm(np.ones((n, n))) == pytest.approx(math.factorial(n), rel=1e-12)
+    assert gpu.perm(np.eye(n)) == pytest.approx(1.0, abs=1e-12)
+    A = np.triu(RNG.uniform(-1, 1, (n, n)))
+    assert gpu.perm(A) == pytest.approx(np.prod(np.diag(A)), rel=1e-10, abs=1e-14)
+    assert gpu.perm(np.ones((n, n)), precision="dd") == pytest.approx(math.factorial(n), rel=1e-15)
+
+
+@pytest.mark.parametrize("k", [1, 2, 4, 6, 8])
+def test_haf_closed_forms(gpu, k):
+    N = 2 * k
+    dfact = math.prod(range(1, N, 2))
+    assert gpu.haf(np.ones((N, N))) == pytest.approx(dfact, rel=1e-12)
+    assert gpu.haf(np.ones((N, N)), precision="dd") == pytest.approx(dfact, rel=1e-15)
+    blocks = np.zeros((N, N))
+    for j in range(k):
+        blocks[2 * j, 2 * j + 1] = blocks[2 * j + 1, 2 * j] = j + 1
+    assert gpu.haf(blocks) == pytest.approx(math.factorial(k), rel=1e-12)
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 6, 9, 12])
+def test_lhaf_closed_forms(gpu, N):
+    telephone = [1, 1, 2, 4, 10, 26, 76, 232, 764, 2620, 9496, 35696, 140152]
+    assert gpu.lhaf(np.ones((N, N))) == pytest.approx(telephone[N], rel=1e-12)
+    d = np.linspace(0.5, 1.5, N)
+    assert gpu.lhaf(np.diag(d)) == pytest.approx(np.prod(d), rel=1e-12)
+    a, b, c = 2.0, 3.0, 5.0
+    assert gpu.lhaf(np.array([[a, b], [b, c]])) == pytest.approx(b + a * c, rel=1e-14)
+
+
+@pytest.mark.parametrize("a", [0.05, 0.3, 0.6])
+@pytest.mark.parametrize("n", [1, 3, 8])
+def test_tor_closed_forms(gpu, a, n):
+    assert gpu.tor(a * np.eye(2 * n)) == pytest.approx((a / (1 - a)) ** n, rel=1e-11)
+    assert gpu.tor(a * np.eye(2 * n), precision="dd") == pytest.approx((a / (1 - a)) ** n, rel=1e-15)
+    assert abs(gpu.tor(np.zeros((2 * n, 2 * n)))) < 1e-12
+
+
+# ---------------------------------------------------------------- against the oracle at larger sizes
+@pytest.mark.parametrize("N", [12, 16, 20])
+def test_haf_vs_binary128_oracle(gpu, orc, N):
+    mats = np.stack([sym(N), sym(N, cplx=False)])
+    for prec, tol in (("fp64", FP64_TOL), ("dd", DD_TOL)):
+        got = gpu.haf_batched(mats, precision=prec)
+        for i in range(2):
+            assert rel_err(got[i], orc.haf(mats[i], "quad")) < tol, (N, prec, i)
+
+
+@pytest.mark.parametrize("N", [11, 16, 20])
+def test_lhaf_vs_binary128_oracle(gpu, orc, N):
+    mats = np.stack([sym(N) for _ in range(2)])
+    for prec, tol in (("fp64", FP64_TOL), ("dd", DD_TOL)):
+        got = gpu.lhaf_batched(mats, precision=prec)
+        for i in range(2):
+            assert rel_err(got[i], orc.lhaf(mats[i], "quad")) < tol, (N, prec, i)
+
+
+@pytest.mark.parametrize("n", [13, 16])
+def test_perm_vs_binary128_oracle(gpu, orc, n):
+    mats = RNG.standard_normal((2, n, n)) + 1j * RNG.standard_normal((2, n, n))
+    for prec, tol in (("fp64", FP64_TOL), ("dd", DD_TOL)):
+        got = gpu.perm_batched(mats, precision=prec)
+        for i in range(2):
+            assert rel_err(got[i], orc.perm(mats[i], "quad")) < tol, (n, prec, i)
+
+
+@pytest.mark.parametrize("n", [6, 11, 14])
+def test_tor_vs_binary128_oracle(gpu, orc, n):
+    mats = np.stack([phys_O(n) for _ in range(2)])
+    for prec, tol in (("fp64", FP64_TOL), ("dd", DD_TOL)):
+        got = gpu.tor_batched(mats, precision=prec)
+        for i in range(2):
+            assert rel_err(got[i], orc.tor(mats[i], "quad")) < tol, (n, prec, i)
+
+
+# ---------------------------------------------------------------- size-independent properties at full sizes
+def test_haf_direct_sum_at_N30(gpu):
+    A, B = sym(14), sym(16)
+    blk = np.zeros((30, 30), dtype=complex)
+    blk[:14, :14], blk[14:, 14:] = A, B
+    h = gpu.haf_batched(np.stack([blk]))[0]
+    assert rel_err(h, gpu.haf(A) * gpu.haf(B)) < 1e-9
+
+
+def test_lhaf_direct_sum_at_N28(gpu):
+    A, B = sym(12), sym(16)
+    blk = np.zeros((28, 28), dtype=complex)
+    blk[:12, :12], blk[12:, 12:] = A, B
+    assert rel_err(gpu.lhaf(blk), gpu.lhaf(A) * gpu.lhaf(B)) < 1e-9
+
+
+def test_perm_direct_sum_at_n28(gpu):
+    A = RNG.standard_normal((14, 14)) + 1j * RNG.standard_normal((14, 14))
+    B = RNG.standard_normal((14, 14)) + 1j * RNG.standard_normal((14, 14))
+    blk = np.zeros((28, 28), dtype=complex)
+    blk[:14, :14], blk[14:, 14:] = A, B
+    assert rel_err(gpu.perm(blk), gpu.perm(A) * gpu.perm(B)) < 1e-9
+
+
+def test_tor_direct_sum_at_24_modes(gpu):
+    O1, O2 = phys_O(12), phys_O(12)
+    n1, n2 = 12, 12
+    n = n1 + n2
+    O = np.zeros((2 * n, 2 * n))
+    idx1 = np.r_[0:n1, n:n + n1]
+    idx2 = np.r_[n1:n, n + n1:2 * n]
+    O[np.ix_(idx1, idx1)] = O1
+    O[np.ix_(idx2, idx2)] = O2
+    assert rel_err(gpu.tor(O), gpu.tor(O1) * gpu.tor(O2)) < 1e-9
+
+
+# ---------------------------------------------------------------- edge cases
+def test_edge_cases(gpu):
+    assert gpu.haf(np.zeros((0, 0))) == 1.0
+    assert gpu.haf(np.ones((5, 5))) == 0.0
+    assert gpu.perm(np.zeros((0, 0))) == 1.0
+    assert gpu.perm(np.array([[3.0 + 1j]])) == 3.0 + 1j
+    assert gpu.lhaf(np.array([[7.0]])) == pytest.approx(7.0)
+    assert gpu.tor(np.zeros((0, 0))) == 1.0
+    for f in ("perm", "haf", "lhaf", "tor"):
+        out = _batched(gpu, f)(np.zeros((0, 4, 4)))
+        assert out.shape == (0,) and out.dtype == np.complex128
+
+
+def test_tor_off_domain_gives_nan(gpu):
+    O = np.stack([phys_O(3), 1.5 * np.eye(6)])  # second: I - O = -0.5 I not SPD
+    v = gpu.tor_batched(O)
+    assert np.isfinite(v[0]) and np.isnan(v[1])
+
+
+# ---------------------------------------------------------------- engineering invariants
+@pytest.mark.parametrize("func", ["perm", "haf", "lhaf", "tor"])
+def test_batched_equals_looped_bitwise(gpu, func):
+    if func == "perm":
+        mats = RNG.standard_normal((5, 9, 9)) + 1j * RNG.standard_normal((5, 9, 9))
+    elif func == "tor":
+        mats = np.stack([phys_O(5) for _ in range(5)])
+    else:
+        mats = np.stack([sym(10) for _ in range(5)])
+    b = _batched(gpu, func)(mats)
+    looped = np.array([getattr(gpu, func)(m) for m in mats])
+    assert np.array_equal(b, looped)
+    assert np.array_equal(b, _batched(gpu, func)(mats))  # deterministic
+
+
+def test_auto_reruns_cancellation_in_dd(gpu):
+    # hafnian family with haf = delta * haf(R): three O(1) matchings cancel to delta
+    # (construction of the reference's bench/_inputs.py cancellation_hafnian)
+    g = np.random.default_rng(5)
+    delta = 1e-9
+    Bk = np.array([[0, 1, 1, 1], [1, 0, delta - 2, 1], [1, delta - 2, 0, 1], [1, 1, 1, 0]], dtype=complex)
+    G2 = g.standard_normal((4, 4))
+    R = G2 + G2.T
+    np.fill_diagonal(R, 0)
+    A = np.zeros((8, 8), dtype=complex)
+    A[:4, :4], A[4:, 4:] = Bk, R
+    delta_exact = 2.0 + (delta - 2.0)  # the hafnian of the binary64 block (Sterbenz-exact)
+    truth = delta_exact * gpu.haf(R, precision="dd")
+    v, d = gpu.haf(A, precision="auto", return_diagnostics=True)
+    assert d["tier"] == "dd" and d["cancellation"] >= 1e8
+    assert rel_err(v, truth) < 1e-12
+    fp = gpu.haf(A)
+    assert rel_err(fp, truth) > rel_err(v, truth)
+
+
+def test_queue_mixed_equals_alone_bitwise(gpu):
+    funcs = ["haf", "lhaf", "tor", "haf", "lhaf", "tor", "haf"]
+    mats = [sym(8), sym(12), phys_O(5), sym(16), sym(7), phys_O(9), sym(2)]
+    precs = ["fp64", "fp64", "fp64", "dd", "kappa", "dd", "fp64"]
+    with gpu.Workspace() as ws:
+        mixed = ws.evaluate(funcs, mats, precs)
+        alone = np.array([ws.evaluate([f], [m], [p])[0] for f, m, p in zip(funcs, mats, precs)])
+    with gpu.Workspace(persistent=False) as ws2:
+        per_size = ws2.evaluate(funcs, mats, precs)
+    assert np.array_equal(mixed, alone)
+    assert np.array_equal(mixed, per_size)
+
+
+def test_workspace_ragged_order_and_reuse(gpu):
+    dims = [4, 6, 4, 8, 6, 4, 8]
+    mats = [sym(d) for d in dims]
+    with gpu.Workspace() as ws:
+        got = ws.haf_batched(mats)
+        for i, m in enumerate(mats):
+            assert got[i] == gpu.haf(m), f"slot {i}"
+        r0 = ws.reallocs
+        ws.haf_batched(mats[:3])
+        assert ws.reallocs == r0  # a smaller batch reuses the resident buffers
+        with pytest.raises(ValueError, match="#1"):
+            ws.haf_batched([np.eye(4), np.zeros((4, 5))])
+        assert ws.haf_batched([]).shape == (0,)
+
+
+def test_workspace_resident_output(gpu):
+    import torch
+    mats = np.stack([sym(10) for _ in range(6)])
+    with gpu.Workspace() as ws:
+        res = ws.haf_resident(mats)
+        host = res.numpy()
+        t = torch.as_tensor(res, device="cuda")
+        assert np.array_equal(host, gpu.haf_batched(mats))
+        assert np.array_equal(t.cpu().numpy(), host)
+        res.close()
