@@ -252,7 +252,9 @@ def main():
     ws = G.Workspace()
     ws.__enter__()
     sess = ws._session
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the launches and the CUDA events that time them share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sptr = ctypes.c_void_p(stream.cuda_stream)
 
     def prepare(mode):

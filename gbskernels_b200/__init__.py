@@ -192,6 +192,10 @@ def _certified_batched(func: str, matrices, rtol: float | None):
             diags.append(d)
     if redo:
         sub = np.ascontiguousarray(stack[redo])
+        if getattr(_lib.load(), f"gbs_{func}_dd_certified_host", None) is None:
+            raise FloatingPointError(
+                f"certified {func}: the fp64 certificate does not reach rtol={rtol} and this "
+                "build has no double-double certificate for it (the mpmath rung is CPU-only)")
         v2, b2 = _call_aux(func, sub, "dd_certified")
         for j, i in enumerate(redo):
             vc, bf = complex(v2[j]), float(b2[j])

@@ -14,6 +14,7 @@
 #include "haf_dd.cuh"
 #include "haf_pt.cuh"
 #include "perm_tor.cuh"
+#include "cert.cuh"
 
 namespace gbsb {
 
@@ -41,6 +42,12 @@ __device__ ItemResult perm_item_n(const double* A2, unsigned long long lo, unsig
     ddc v = ddc{dd_make(0.0), dd_make(0.0)};
     if (active) v = perm_lane_range_dd<NN>(A2, i0, R);
     r.val = warp_sum_ddc(v);
+  } else if (TIER == kTierCert) {
+    cball b{mkc(0.0, 0.0), 0.0};
+    if (active) b = perm_lane_range_cert<NN>(A2, i0, R);
+    b = warp_sum_cb(b);
+    r.val = ddc_from_c(b.z);
+    r.aux = b.r;
   } else {
     double absacc = 0.0;
     cplx v = mkc(0.0, 0.0);
@@ -92,12 +99,22 @@ __device__ ItemResult haf_item(const double* __restrict__ mats, const InstDesc& 
       acc = ddc_add(acc, t);
     }
     r.val = acc;
+  } else if (TIER == kTierCert) {
+    const HafLayout L = haf_layout(haf_smax, true);
+    cball acc{mkc(0.0, 0.0), 0.0};
+    for (unsigned long long k = 0; k < w.count; ++k) {
+      cball t = haf_subset_term_tc<true>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      acc = cb_add(acc, t);
+    }
+    r.val = ddc_from_c(acc.z);
+    r.aux = acc.r;
+    if (!isfinite(acc.r) || !isfinite(acc.z.re) || !isfinite(acc.z.im)) r.st = kStUncertified;
   } else {
     const HafLayout L = haf_layout(haf_smax);
     cplx acc = mkc(0.0, 0.0);
     double absacc = 0.0;
     for (unsigned long long k = 0; k < w.count; ++k) {
-      cplx t = haf_subset_term_tc(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      cplx t = haf_subset_term_tc<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane).z;
       acc = cadd(acc, t);
       if (TIER == kTierKappa) absacc += cabs_fast(t);
     }
@@ -121,7 +138,17 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
   const uint32_t pat = (uint32_t)(w.lo + lane);
   bool ok = true;
   double absacc = 0.0;
-  if (TIER == kTierDD) {
+  if (TIER == kTierCert) {
+    double total = 0.0, bnd = 0.0;
+    if (active) {
+      double L[kTorPackedMax], EL[kTorPackedMax];
+      ok = tor_lane_subtree_cert(ws, n, d.param, pat, L, EL, total, bnd);
+    }
+    cball b{mkc(ok ? total : 0.0, 0.0), ok ? bnd : 0.0};
+    b = warp_sum_cb(b);
+    r.val = ddc{dd_make(b.z.re), dd_make(0.0)};
+    r.aux = b.r;
+  } else if (TIER == kTierDD) {
     dd total = dd_make(0.0);
     if (active) {
       dd L[kTorPackedMax];
@@ -142,7 +169,7 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
     r.aux = warp_sum_d(absacc);
   }
   const bool all_ok = __all_sync(0xffffffffu, ok);
-  if (!all_ok) r.st = kStOffDomain;
+  if (!all_ok) r.st = TIER == kTierCert ? kStUncertified : kStOffDomain;
   __syncwarp();
   return r;
 }
@@ -169,6 +196,10 @@ __device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstD
     GBSB_BR(kFnTor, kTierFp64, (tor_item<kTierFp64>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierKappa, (tor_item<kTierKappa>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierDD, (tor_item<kTierDD>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnPerm, kTierCert, (perm_item<kTierCert>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnHaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, false, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnLhaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnTor, kTierCert, (tor_item<kTierCert>(P.mats, d, w, ws, lane)))
 #undef GBSB_BR
     default:
       break;
@@ -206,18 +237,22 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
       __threadfence();
       // Deterministic reduction: lane l sums items l, l+32, ... in order, then a
       // fixed butterfly combines the lanes.  Partials are read through L2.
+      const bool cert = (d.ft & 3) == kTierCert;
       ddc acc = ddc{dd_make(0.0), dd_make(0.0)};
-      double aux = 0.0;
+      double aux = 0.0, mag = 0.0;
       int st = kStOk;
       for (int k = lane; k < d.nitems; k += 32) {
         const double* pp = P.part + (size_t)(d.item0 + k) * 4;
         ddc v = ddc{dd{__ldcg(pp), __ldcg(pp + 1)}, dd{__ldcg(pp + 2), __ldcg(pp + 3)}};
         acc = ddc_add(acc, v);
-        aux += __ldcg(P.paux + d.item0 + k);
+        const double a = __ldcg(P.paux + d.item0 + k);
+        aux = cert ? ru_add(aux, a) : aux + a;
+        if (cert) mag = ru_add(mag, ru_abs_c(cplx{v.re.hi, v.im.hi}));
         st = max(st, __ldcg(P.pst + d.item0 + k));
       }
       acc = warp_sum_ddc(acc);
-      aux = warp_sum_d(aux);
+      aux = cert ? warp_sum_ru(aux) : warp_sum_d(aux);
+      if (cert) mag = warp_sum_ru(mag);
 #pragma unroll
       for (int m = 16; m > 0; m >>= 1) st = max(st, __shfl_xor_sync(0xffffffffu, st, m));
       if (lane == 0) {
@@ -226,9 +261,18 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
         if (fn == kFnPerm && d.dim > 0) {
           const double sc = ldexp(1.0, -(d.dim - 1));  // 1 / 2^(n-1), exact
           v = cscale(v, sc);
-          aux *= sc;
+          if (!cert) aux *= sc;
         }
-        if (st == kStOffDomain) v = mkc(NAN, NAN);
+        if (cert) {
+          // double-word summation of the partials (relative error < 2^-100 per step,
+          // d.nitems + 5 steps) plus the final rounding to binary64
+          const double dsum = ru_mul(ru_mul((double)(d.nitems + 6), 7.888609052210118e-31), mag);
+          aux = ru_add(aux, dsum);
+          if (fn == kFnPerm) aux = ru_mul(aux, ldexp(1.0, -(d.dim - 1)));  // v is already scaled
+          aux = ru_add(aux, ru_add(ru_mul(kUc, ru_abs_c(v)), kUfl));
+          if (!isfinite(aux)) st = max(st, (int)kStUncertified);
+        }
+        if (st != kStOk) { v = mkc(NAN, NAN); if (cert) aux = INFINITY; }
         P.out[2 * (size_t)w.inst] = v.re;
         P.out[2 * (size_t)w.inst + 1] = v.im;
         P.aux_out[w.inst] = aux;

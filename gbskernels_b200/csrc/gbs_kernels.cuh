@@ -41,9 +41,10 @@ struct WorkItem {       // 24 bytes
 // smallest compiled set covering the (function, tier) pairs of its batch.
 constexpr unsigned br1(int fn, int tier) { return 1u << ft_code(fn, tier); }
 constexpr unsigned kBrHafLhafFp64 = br1(kFnHaf, kTierFp64) | br1(kFnLhaf, kTierFp64);
-// haf / lhaf / tor in fp64 and fp64+indicator: the serving mix
+// haf / lhaf / tor in fp64, fp64 + indicator and certified: the serving mix
 constexpr unsigned kBrServe = kBrHafLhafFp64 | br1(kFnTor, kTierFp64) | br1(kFnHaf, kTierKappa) |
-                              br1(kFnLhaf, kTierKappa) | br1(kFnTor, kTierKappa);
+                              br1(kFnLhaf, kTierKappa) | br1(kFnTor, kTierKappa) | br1(kFnHaf, kTierCert) |
+                              br1(kFnLhaf, kTierCert) | br1(kFnTor, kTierCert);
 // haf / lhaf / tor in every tier
 constexpr unsigned kBrMixed = kBrServe | br1(kFnHaf, kTierDD) | br1(kFnLhaf, kTierDD) | br1(kFnTor, kTierDD);
 

@@ -13,19 +13,25 @@
 // B200 mapping (this repository's own design):
 //   * One warp evaluates one subset at a time; C (s x s complex, s = 2|S|) is
 //     staged in shared memory.
-//   * Row strips of 16 rows evolve independently: strip(C^{a+1}) = strip(C^a) C.
-//     The complex product runs on the FP64 tensor cores through the real
-//     embedding  [Re P, Im P] (interleaved) x B',  B'[2k+p][2j+q] = (p ? iC : C)[k][j]
-//     component (q ? im : re), so one m16n8k4 mma consumes two complex columns.
+//   * All 16-row strips of C^a advance together: C^{a+1} = C^a C on the FP64 tensor
+//     cores through the real embedding [Re P, Im P] (interleaved) x B',
+//     B'[2k+p][2j+q] = (p ? iC : C)[k][j] component (q ? im : re): one m16n8k4 mma
+//     consumes two complex columns; each B' fragment is loaded once and used by
+//     every strip; with few tiles the K loop is split into two accumulator sets so
+//     at least eight independent mma chains are in flight.
 //   * Since C^T = X C X (B_S symmetric), (C^a)^T = X C^a X and
 //       tr(C^{2a})   = sum_{i,t} C^a[i][t]     C^a[i^1][t^1]
 //       tr(C^{2a-1}) = sum_{i,t} C^a[i][t] C^{a-1}[i^1][t^1],
 //     so powers up to h = ceil(n/2) give every trace p_1..p_n: h-1 products per
-//     subset instead of the reference's n-1.  Rows i and i^1 share a strip.
+//     subset instead of the reference's n-1.  In the mma accumulator layout the
+//     partner element (i^1, t^1) of a lane's element sits in lane ^ 5, same
+//     register: the even trace is a shuffle, the odd one reads the previous power,
+//     which is then overwritten in place.
 //   * Loop term: with y_a = C^a d, d^T X C^{a+b} d = (X y_a)^T y_b, so
 //     v_k = (1/2) sum_i y_a[i^1] y_b[i] with a + b = k - 1 from the same powers.
 #pragma once
 
+#include "cert.cuh"
 #include "gbs_common.cuh"
 
 namespace gbsb {
@@ -37,136 +43,347 @@ constexpr int kHafMaxPow = (kHafMaxPairs + 1) / 2;  // h
 // Strides (in complex elements) chosen for conflict-free fragment loads.
 __host__ __device__ inline int haf_c_stride(int s) { return ((s + 3) / 8) * 8 + 4; }   // == 4 (mod 8)
 __host__ __device__ inline int haf_p_stride(int s) { return (s % 4 == 2) ? s : s + 2; }  // == 2 (mod 4)
+__host__ __device__ inline int haf_strips(int s) { return (s + 15) / 16; }
 
 // Per-warp shared-memory workspace (doubles), laid out for a launch-wide max s.
 struct HafLayout {
   int smax;
-  int c_off, p0_off, p1_off, y_off, d_off, gi_off, acc_off, total;  // in doubles
+  int c_off, p_off, y_off, d_off, gi_off, acc_off, total;  // in doubles
+  // certified tier only: |C|, the bound-path power, row bounds and trace-bound sums
+  int ca_off, m_off, ym_off, bt_off;
 };
-__host__ __device__ inline HafLayout haf_layout(int smax) {
+__host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   HafLayout L;
   if (smax < 2) smax = 2;
   L.smax = smax;
-  int cs = haf_c_stride(smax), ps = haf_p_stride(smax);
-  int h = (smax / 2 + 1) / 2;
+  const int cs = haf_c_stride(smax), ps = haf_p_stride(smax);
+  const int rows = 16 * haf_strips(smax);
+  const int h = (smax / 2 + 1) / 2;
   L.c_off = 0;
-  L.p0_off = L.c_off + smax * cs * 2;
-  L.p1_off = L.p0_off + 16 * ps * 2;
-  L.y_off = L.p1_off + 16 * ps * 2;
-  L.d_off = L.y_off + 16 * (h + 1) * 2;
+  L.p_off = L.c_off + smax * cs * 2;
+  L.y_off = L.p_off + rows * ps * 2;
+  L.d_off = L.y_off + rows * (h + 1) * 2;
   L.gi_off = L.d_off + 32 * 2;   // 32 ints
   L.acc_off = L.gi_off + 16;
-  // acc: p[0..n], v[0..n], kg/e scratch [0..n] x 2  -> 4 * (kHafMaxPairs+1) complex
   L.total = L.acc_off + 4 * (kHafMaxPairs + 1) * 2;
   L.total = (L.total + 1) & ~1;  // 16-byte multiple
+  L.ca_off = L.m_off = L.ym_off = L.bt_off = 0;
+  if (cert) {
+    L.ca_off = L.total;
+    L.m_off = L.ca_off + smax * cs * 2;
+    L.ym_off = L.m_off + rows * ps * 2;
+    L.bt_off = L.ym_off + rows * (h + 1);
+    L.total = L.bt_off + 2 * (kHafMaxPairs + 2);
+    L.total = (L.total + 1) & ~1;
+  }
   return L;
 }
 
 // ---------------------------------------------------------------------------
-// One strip product  P1[0:16][0:s] = P0[0:16][0:s] * C   (complex), NT n-tiles.
-template <int NT>
-__device__ __forceinline__ void strip_product(const double* __restrict__ P0, double* __restrict__ P1,
-                                              const double* __restrict__ Cs, int s, int cs, int ps,
-                                              int lane) {
+// D = P * C for every strip of P (rows 16 MS, complex), accumulators in the mma
+// layout: D[ms][nt][0..3] = rows (16ms+g, 16ms+g+8), complex column 4nt+t4 (re, im).
+template <int NT, int MS>
+__device__ __forceinline__ void power_product(const double* __restrict__ P, const double* __restrict__ Cs, int s,
+                                              int cs, int ps, int lane, double (&D)[MS][NT][4]) {
+  constexpr int KS2 = (NT * MS < 8) ? 2 : 1;  // split K when few tiles are in flight
   const int g = lane >> 2, t4 = lane & 3;
-  double d[NT][4];
+  double acc[KS2][MS][NT][4];
 #pragma unroll
-  for (int nt = 0; nt < NT; ++nt) d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.0;
-  // B' fragment address for this lane: C[k][j] component (p ^ q), negated when p & !q,
-  // with k = 2 ks + (t4 >> 1), p = t4 & 1, j = 4 nt + (g >> 1), q = g & 1.
+  for (int k2 = 0; k2 < KS2; ++k2)
+#pragma unroll
+    for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+        acc[k2][ms][nt][0] = acc[k2][ms][nt][1] = acc[k2][ms][nt][2] = acc[k2][ms][nt][3] = 0.0;
+  // B' fragment of this lane: C[k][j] component (p ^ q), negated when p & !q, with
+  // k = 2 ks + (t4 >> 1), p = t4 & 1, j = 4 nt + (g >> 1), q = g & 1.
   const double* bptr = Cs + ((t4 >> 1) * cs + (g >> 1)) * 2 + ((t4 ^ g) & 1);
   const unsigned long long sgn = ((t4 & 1) && !(g & 1)) ? 0x8000000000000000ull : 0ull;
-  const double* a0p = P0 + g * ps * 2 + t4;
-  const double* a1p = P0 + (g + 8) * ps * 2 + t4;
-  const int ks_n = s >> 1;  // K = 2s real columns, 4 per slice
-#pragma unroll 2
-  for (int ks = 0; ks < ks_n; ++ks) {
-    const double a0 = a0p[4 * ks];
-    const double a1 = a1p[4 * ks];
+  const double* ap = P + g * ps * 2 + t4;
+  const int ksn = s >> 1;  // K = 2s real columns, 4 per slice
+  auto slice = [&](int ks, int k2) {
+    double a0[MS], a1[MS];
+#pragma unroll
+    for (int ms = 0; ms < MS; ++ms) {
+      a0[ms] = ap[(16 * ms) * ps * 2 + 4 * ks];
+      a1[ms] = ap[(16 * ms + 8) * ps * 2 + 4 * ks];
+    }
     const double* bp = bptr + ks * 4 * cs;
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-      double b = __longlong_as_double(__double_as_longlong(bp[nt * 8]) ^ sgn);
-      dmma_m16n8k4(d[nt], a0, a1, b);
-    }
-  }
+      const double b = __longlong_as_double(__double_as_longlong(bp[nt * 8]) ^ sgn);
 #pragma unroll
-  for (int nt = 0; nt < NT; ++nt) {
-    const int col = 4 * nt + t4;  // complex column held by this lane
-    if (col < s) {
-      double2* r0 = reinterpret_cast<double2*>(P1 + (g * ps + col) * 2);
-      double2* r1 = reinterpret_cast<double2*>(P1 + ((g + 8) * ps + col) * 2);
-      *r0 = make_double2(d[nt][0], d[nt][1]);
-      *r1 = make_double2(d[nt][2], d[nt][3]);
+      for (int ms = 0; ms < MS; ++ms) dmma_m16n8k4(acc[k2][ms][nt], a0[ms], a1[ms], b);
+    }
+  };
+  if constexpr (KS2 == 2) {
+    int ks = 0;
+#pragma unroll 1
+    for (; ks + 1 < ksn; ks += 2) {
+      slice(ks, 0);
+      slice(ks + 1, 1);
+    }
+    if (ks < ksn) slice(ks, 0);
+#pragma unroll
+    for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) D[ms][nt][q] = acc[0][ms][nt][q] + acc[KS2 - 1][ms][nt][q];
+  } else {
+#pragma unroll 2
+    for (int ks = 0; ks < ksn; ++ks) slice(ks, 0);
+#pragma unroll
+    for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) D[ms][nt][q] = acc[0][ms][nt][q];
+  }
+}
+
+// Load P (power a, complex, stride ps) into the accumulator layout.
+template <int NT, int MS>
+__device__ __forceinline__ void load_acc(const double* P, int ps, int s, int lane, double (&D)[MS][NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int col = 4 * nt + t4;
+      cplx x0 = mkc(0.0, 0.0), x1 = mkc(0.0, 0.0);
+      if (col < s) {
+        x0 = ld_c(P + ((16 * ms + g) * ps + col) * 2);
+        x1 = ld_c(P + ((16 * ms + g + 8) * ps + col) * 2);
+      }
+      D[ms][nt][0] = x0.re; D[ms][nt][1] = x0.im; D[ms][nt][2] = x1.re; D[ms][nt][3] = x1.im;
+    }
+}
+
+// Store the accumulators into P (rows < 16 MS, columns < s).
+template <int NT, int MS>
+__device__ __forceinline__ void store_acc(double* P, int ps, int s, int lane, const double (&D)[MS][NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int col = 4 * nt + t4;
+      if (col < s) {
+        st_c(P + ((16 * ms + g) * ps + col) * 2, mkc(D[ms][nt][0], D[ms][nt][1]));
+        st_c(P + ((16 * ms + g + 8) * ps + col) * 2, mkc(D[ms][nt][2], D[ms][nt][3]));
+      }
+    }
+}
+
+// Lane partial of sum_{i,t} D[i][t] * D[i^1][t^1] (partner in lane ^ 5, same slot).
+template <int NT, int MS>
+__device__ __forceinline__ cplx even_partial(const double (&D)[MS][NT][4]) {
+  cplx acc = mkc(0.0, 0.0);
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const double p0 = shfl_xor_d(D[ms][nt][0], 5), p1 = shfl_xor_d(D[ms][nt][1], 5);
+      const double p2 = shfl_xor_d(D[ms][nt][2], 5), p3 = shfl_xor_d(D[ms][nt][3], 5);
+      acc = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), mkc(p0, p1), acc);
+      acc = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), mkc(p2, p3), acc);
+    }
+  return acc;
+}
+
+// Lane partial of sum_{i,t} D[i][t] * Q[i^1][t^1], Q the previous power in shared memory.
+template <int NT, int MS>
+__device__ __forceinline__ cplx odd_partial(const double (&D)[MS][NT][4], const double* Q, int ps, int s,
+                                            int lane) {
+  const int g = lane >> 2, t4 = lane & 3;
+  cplx acc = mkc(0.0, 0.0);
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int col = 4 * nt + t4;
+      if (col < s) {
+        const int cp = col ^ 1;
+        const cplx q0 = ld_c(Q + ((16 * ms + (g ^ 1)) * ps + cp) * 2);
+        const cplx q1 = ld_c(Q + ((16 * ms + ((g + 8) ^ 1)) * ps + cp) * 2);
+        acc = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), q0, acc);
+        acc = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), q1, acc);
+      }
+    }
+  return acc;
+}
+
+// y[row] = sum_t D[row][t] d[t] for the rows of this lane's group; lanes t4 == 0
+// write Y[row * hp1 + col].
+template <int NT, int MS>
+__device__ __forceinline__ void rows_times_d(const double (&D)[MS][NT][4], const double* Dv, double* Y, int col,
+                                             int hp1, int s, int lane) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms) {
+    cplx y0 = mkc(0.0, 0.0), y1 = mkc(0.0, 0.0);
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int c = 4 * nt + t4;
+      if (c < s) {
+        const cplx dv = ld_c(Dv + c * 2);
+        y0 = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), dv, y0);
+        y1 = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), dv, y1);
+      }
+    }
+#pragma unroll
+    for (int m = 1; m <= 2; m <<= 1) {
+      y0.re += shfl_xor_d(y0.re, m); y0.im += shfl_xor_d(y0.im, m);
+      y1.re += shfl_xor_d(y1.re, m); y1.im += shfl_xor_d(y1.im, m);
+    }
+    if (t4 == 0) {
+      st_c(Y + ((16 * ms + g) * hp1 + col) * 2, y0);
+      st_c(Y + ((16 * ms + g + 8) * hp1 + col) * 2, y1);
     }
   }
 }
 
-__device__ __forceinline__ void strip_product_dispatch(const double* P0, double* P1, const double* Cs,
-                                                       int s, int cs, int ps, int lane) {
-  switch ((2 * s + 7) >> 3) {
-    case 1: strip_product<1>(P0, P1, Cs, s, cs, ps, lane); break;
-    case 2: strip_product<2>(P0, P1, Cs, s, cs, ps, lane); break;
-    case 3: strip_product<3>(P0, P1, Cs, s, cs, ps, lane); break;
-    case 4: strip_product<4>(P0, P1, Cs, s, cs, ps, lane); break;
-    case 5: strip_product<5>(P0, P1, Cs, s, cs, ps, lane); break;
-    case 6: strip_product<6>(P0, P1, Cs, s, cs, ps, lane); break;
-    case 7: strip_product<7>(P0, P1, Cs, s, cs, ps, lane); break;
-    default: strip_product<8>(P0, P1, Cs, s, cs, ps, lane); break;
+// ---- bound path helpers (certified tier): real parts only, upward rounding
+template <int NT, int MS>
+__device__ __forceinline__ double even_bound(const double (&D)[MS][NT][4]) {
+  double acc = 0.0;
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      acc = ru_fma(D[ms][nt][0], shfl_xor_d(D[ms][nt][0], 5), acc);
+      acc = ru_fma(D[ms][nt][2], shfl_xor_d(D[ms][nt][2], 5), acc);
+    }
+  return acc;
+}
+template <int NT, int MS>
+__device__ __forceinline__ double odd_bound(const double (&D)[MS][NT][4], const double* Q, int ps, int s, int lane) {
+  const int g = lane >> 2, t4 = lane & 3;
+  double acc = 0.0;
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int col = 4 * nt + t4;
+      if (col < s) {
+        const int cp = col ^ 1;
+        acc = ru_fma(D[ms][nt][0], Q[((16 * ms + (g ^ 1)) * ps + cp) * 2], acc);
+        acc = ru_fma(D[ms][nt][2], Q[((16 * ms + ((g + 8) ^ 1)) * ps + cp) * 2], acc);
+      }
+    }
+  return acc;
+}
+template <int NT, int MS>
+__device__ __forceinline__ void rows_bound(const double (&D)[MS][NT][4], const double* Dv, double* Ym, int col,
+                                           int hp1, int s, int lane) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int ms = 0; ms < MS; ++ms) {
+    double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int c = 4 * nt + t4;
+      if (c < s) {
+        const double dv = ru_abs_c(ld_c(Dv + c * 2));
+        y0 = ru_fma(D[ms][nt][0], dv, y0);
+        y1 = ru_fma(D[ms][nt][2], dv, y1);
+      }
+    }
+#pragma unroll
+    for (int m = 1; m <= 2; m <<= 1) {
+      y0 = ru_add(y0, shfl_xor_d(y0, m));
+      y1 = ru_add(y1, shfl_xor_d(y1, m));
+    }
+    if (t4 == 0) {
+      Ym[(16 * ms + g) * hp1 + col] = y0;
+      Ym[(16 * ms + g + 8) * hp1 + col] = y1;
+    }
   }
 }
 
-
-// sum over the strip's valid rows i and columns t of X[i][t] * Y[i^1][t^1].
-__device__ __forceinline__ cplx strip_pair_trace(const double* X, const double* Y, int rows, int s,
-                                                 int ps, int lane) {
-  cplx acc = mkc(0.0, 0.0);
-  const int tot = rows * s;
-  for (int e = lane; e < tot; e += 32) {
-    int i = e / s, t = e - i * s;
-    acc = cfma(ld_c(X + (i * ps + t) * 2), ld_c(Y + ((i ^ 1) * ps + (t ^ 1)) * 2), acc);
+// ---------------------------------------------------------------------------
+// Power loop of one subset for the compile-time tile shape (NT column tiles of 8
+// real columns, MS strips of 16 rows).  Accumulates the traces into acc_p[k], the
+// loop vectors into Y and (certified) the trace / row bound sums into bT / Ym.
+template <int NT, int MS, bool CERT>
+__device__ __forceinline__ void haf_powers(const double* Cs, double* P, double* Y, const double* Dv, double* acc_p,
+                                           const double* Ca, double* M, double* Ym, double* bT, int s, int cs, int ps,
+                                           int n, int h, bool loop, int lane) {
+  const int hp1 = h + 1;
+  double D[MS][NT][4];
+  // power 1 (P = C): p_2 and y_1
+  load_acc<NT, MS>(P, ps, s, lane, D);
+  {
+    cplx t = warp_sum_c(even_partial<NT, MS>(D));
+    if (lane == 0 && 2 <= n) st_c(acc_p + 4, cadd(ld_c(acc_p + 4), t));
   }
-  return warp_sum_c(acc);
-}
-
-// Loop-term vectors y[i] = sum_t P[i][t] d[t] for the strip rows (lanes 2i, 2i+1 split t).
-__device__ __forceinline__ void strip_matvec(const double* P, const double* dv, double* y, int rows,
-                                             int s, int ps, int lane) {
-  const int i = lane >> 1, half = lane & 1;
-  cplx acc = mkc(0.0, 0.0);
-  if (i < rows) {
-    for (int t = half; t < s; t += 2) acc = cfma(ld_c(P + (i * ps + t) * 2), ld_c(dv + t * 2), acc);
+  if (loop) rows_times_d<NT, MS>(D, Dv, Y, 1, hp1, s, lane);
+  if constexpr (CERT) {
+    double Dm[MS][NT][4];
+    load_acc<NT, MS>(M, ps, s, lane, Dm);
+    double tb = warp_sum_ru(even_bound<NT, MS>(Dm));
+    if (lane == 0 && 2 <= n) bT[2] = ru_add(bT[2], tb);
+    if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, 1, hp1, s, lane);
   }
-  acc.re += shfl_xor_d(acc.re, 1);
-  acc.im += shfl_xor_d(acc.im, 1);
-  if (half == 0 && i < 16) st_c(y + i * 2, i < rows ? acc : mkc(0.0, 0.0));
+  for (int a = 2; a <= h; ++a) {
+    power_product<NT, MS>(P, Cs, s, cs, ps, lane, D);
+    cplx to = warp_sum_c(odd_partial<NT, MS>(D, P, ps, s, lane));
+    cplx te = warp_sum_c(even_partial<NT, MS>(D));
+    if (lane == 0) {
+      if (2 * a - 1 <= n) st_c(acc_p + 2 * (2 * a - 1), cadd(ld_c(acc_p + 2 * (2 * a - 1)), to));
+      if (2 * a <= n) st_c(acc_p + 2 * (2 * a), cadd(ld_c(acc_p + 2 * (2 * a)), te));
+    }
+    __syncwarp();
+    store_acc<NT, MS>(P, ps, s, lane, D);
+    if (loop) rows_times_d<NT, MS>(D, Dv, Y, a, hp1, s, lane);
+    if constexpr (CERT) {
+      double Dm[MS][NT][4];
+      power_product<NT, MS>(M, Ca, s, cs, ps, lane, Dm);
+      double bo = warp_sum_ru(odd_bound<NT, MS>(Dm, M, ps, s, lane));
+      double be = warp_sum_ru(even_bound<NT, MS>(Dm));
+      if (lane == 0) {
+        if (2 * a - 1 <= n) bT[2 * a - 1] = ru_add(bT[2 * a - 1], bo);
+        if (2 * a <= n) bT[2 * a] = ru_add(bT[2 * a], be);
+      }
+      __syncwarp();
+      store_acc<NT, MS>(M, ps, s, lane, Dm);
+      if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, a, hp1, s, lane);
+    }
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Evaluate the signed power-trace term of one subset `mask` of instance A (N x N
-// complex, row-major, N = 2n even).  Returns the same value in every lane.
-// `loop` selects the loop hafnian.  `ws` is this warp's shared workspace.
-static __device__ cplx haf_subset_term_tc(const double* __restrict__ A, int N, int n, uint32_t mask,
-                                   bool loop, double* ws, const HafLayout& Lw, int lane) {
+// complex, row-major, N = 2n even).  Returns the same ball in every lane (radius 0
+// unless CERT).  `loop` selects the loop hafnian; `ws` is this warp's workspace.
+template <bool CERT>
+static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, int n, uint32_t mask,
+                                           bool loop, double* ws, const HafLayout& Lw, int lane) {
   const int m = __popc(mask);
-  if (m == 0) return mkc(n == 0 ? 1.0 : 0.0, 0.0);
+  if (m == 0) return cball{mkc(n == 0 ? 1.0 : 0.0, 0.0), 0.0};
   const int s = 2 * m;
   const int cs = haf_c_stride(s), ps = haf_p_stride(s);
-  const int h = (n + 1) / 2;
+  const int h = (n + 1) / 2, hp1 = h + 1;
+  const int rows = 16 * haf_strips(s);
   double* Cs = ws + Lw.c_off;
-  double* P0 = ws + Lw.p0_off;
-  double* P1 = ws + Lw.p1_off;
-  double* Y = ws + Lw.y_off;        // [16 rows][h+1] complex, row-major by power
+  double* P = ws + Lw.p_off;
+  double* Y = ws + Lw.y_off;        // [rows][h+1] complex
   double* Dv = ws + Lw.d_off;       // d[0..s)
+  int* gi = reinterpret_cast<int*>(ws + Lw.gi_off);
   double* acc_p = ws + Lw.acc_off;  // p[0..n]
   double* acc_v = acc_p + (kHafMaxPairs + 1) * 2;
   double* kg = acc_v + (kHafMaxPairs + 1) * 2;
   double* ev = kg + (kHafMaxPairs + 1) * 2;
+  double* Ca = ws + Lw.ca_off;
+  double* M = ws + Lw.m_off;
+  double* Ym = ws + Lw.ym_off;
+  double* bT = ws + Lw.bt_off;                  // trace bound sums T[k]
+  double* bV = bT + (kHafMaxPairs + 2);         // loop bound sums V[k]
 
-  // ---- stage C = B_S X (and d) in shared memory.  gi[r] = global row of local row r.
-  int* gi = reinterpret_cast<int*>(ws + Lw.gi_off);
+  // ---- stage C = B_S X, d, and P = C (rows padded to 16 MS with zeros)
   if (lane < s) {
-    // position of the (lane/2)-th set bit of mask
     uint32_t mm = mask;
     for (int u = 0; u < (lane >> 1); ++u) mm &= mm - 1;
     gi[lane] = 2 * (__ffs(mm) - 1) + (lane & 1);
@@ -174,118 +391,152 @@ static __device__ cplx haf_subset_term_tc(const double* __restrict__ A, int N, i
   __syncwarp();
   const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
   for (int e = lane; e < s * ccols; e += 32) {
-    int r = e / ccols, c = e - r * ccols;
+    const int r = e / ccols, c = e - r * ccols;
     cplx v = mkc(0.0, 0.0);
     if (c < s) {
-      int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
+      const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
       if (loop || rr != cc) v = ld_c(A + ((size_t)rr * N + cc) * 2);
     }
     st_c(Cs + (r * cs + c) * 2, v);
+    if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
   }
-  if (loop && lane < s) {
-    int rr = gi[lane];
-    st_c(Dv + lane * 2, ld_c(A + ((size_t)rr * N + rr) * 2));
+  __syncwarp();
+  for (int e = lane; e < rows * ps; e += 32) {
+    const int r = e / ps, c = e - r * ps;
+    const bool in = r < s && c < s;
+    st_c(P + e * 2, in ? ld_c(Cs + (r * cs + c) * 2) : mkc(0.0, 0.0));
+    if constexpr (CERT) st_c(M + e * 2, in ? ld_c(Ca + (r * cs + c) * 2) : mkc(0.0, 0.0));
   }
+  if (loop && lane < s) st_c(Dv + lane * 2, ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2));
   for (int k = lane; k <= n; k += 32) {
     st_c(acc_p + 2 * k, mkc(0.0, 0.0));
     st_c(acc_v + 2 * k, mkc(0.0, 0.0));
+    if constexpr (CERT) { bT[k] = 0.0; bV[k] = 0.0; }
   }
   __syncwarp();
-
+  if (loop && lane < rows) {
+    st_c(Y + (lane * hp1) * 2, lane < s ? ld_c(Dv + lane * 2) : mkc(0.0, 0.0));  // y_0 = d
+    if constexpr (CERT) Ym[lane * hp1] = lane < s ? ru_abs_c(ld_c(Dv + lane * 2)) : 0.0;
+  }
   // p_1 = tr(C)
   {
     cplx t = mkc(0.0, 0.0);
     if (lane < s) t = ld_c(Cs + (lane * cs + lane) * 2);
     t = warp_sum_c(t);
     if (lane == 0) st_c(acc_p + 2, t);
+    if constexpr (CERT) {
+      double a1 = lane < s ? ru_abs_c(ld_c(Cs + (lane * cs + lane) * 2)) : 0.0;
+      a1 = warp_sum_ru(a1);
+      if (lane == 0) bT[1] = a1;
+    }
   }
+  __syncwarp();
 
-  const int nstrips = (s + 15) >> 4;
-  for (int st = 0; st < nstrips; ++st) {
-    const int r0 = st * 16;
-    const int rows = min(16, s - r0);
-    double* Pa = P0;  // power a-1 (after swap: current)
-    double* Pb = P1;
-    // P0 <- C rows of the strip (rows beyond s zero; both buffers zero-padded)
-    for (int e = lane; e < 16 * ps; e += 32) {
-      int i = e / ps, t = e - i * ps;
-      cplx v = (i < rows && t < s) ? ld_c(Cs + ((r0 + i) * cs + t) * 2) : mkc(0.0, 0.0);
-      st_c(Pa + e * 2, v);
-      st_c(Pb + e * 2, mkc(0.0, 0.0));
-    }
-    __syncwarp();
-    // power 1: p_2 = self trace; loop: y_0 = d, y_1 = C d
-    {
-      cplx t = strip_pair_trace(Pa, Pa, rows, s, ps, lane);
-      if (lane == 0 && 2 <= n) st_c(acc_p + 4, cadd(ld_c(acc_p + 4), t));
-    }
-    if (loop) {
-      if (lane < 16) st_c(Y + (lane * (h + 1) + 0) * 2, lane < rows ? ld_c(Dv + (r0 + lane) * 2) : mkc(0.0, 0.0));
-      // y_1 rows -> Y[i][1]
-      {
-        const int i = lane >> 1, half = lane & 1;
-        cplx acc = mkc(0.0, 0.0);
-        if (i < rows)
-          for (int t = half; t < s; t += 2) acc = cfma(ld_c(Pa + (i * ps + t) * 2), ld_c(Dv + t * 2), acc);
-        acc.re += shfl_xor_d(acc.re, 1);
-        acc.im += shfl_xor_d(acc.im, 1);
-        if (half == 0 && i < 16) st_c(Y + (i * (h + 1) + 1) * 2, i < rows ? acc : mkc(0.0, 0.0));
-      }
-    }
-    __syncwarp();
-    for (int a = 2; a <= h; ++a) {
-      strip_product_dispatch(Pa, Pb, Cs, s, cs, ps, lane);
-      __syncwarp();
-      // p_{2a-1} = tr(C^a C^{a-1}),  p_{2a} = tr(C^a C^a)
-      cplx todd = strip_pair_trace(Pb, Pa, rows, s, ps, lane);
-      cplx tev = strip_pair_trace(Pb, Pb, rows, s, ps, lane);
-      if (lane == 0) {
-        if (2 * a - 1 <= n) st_c(acc_p + 2 * (2 * a - 1), cadd(ld_c(acc_p + 2 * (2 * a - 1)), todd));
-        if (2 * a <= n) st_c(acc_p + 2 * (2 * a), cadd(ld_c(acc_p + 2 * (2 * a)), tev));
-      }
-      if (loop) {
-        const int i = lane >> 1, half = lane & 1;
-        cplx acc = mkc(0.0, 0.0);
-        if (i < rows)
-          for (int t = half; t < s; t += 2) acc = cfma(ld_c(Pb + (i * ps + t) * 2), ld_c(Dv + t * 2), acc);
-        acc.re += shfl_xor_d(acc.re, 1);
-        acc.im += shfl_xor_d(acc.im, 1);
-        if (half == 0 && i < 16) st_c(Y + (i * (h + 1) + a) * 2, i < rows ? acc : mkc(0.0, 0.0));
-      }
-      __syncwarp();
-      double* tmp = Pa; Pa = Pb; Pb = tmp;
-    }
-    if (loop) {
-      // v_k += 1/2 sum_i y_a[i^1] y_b[i],  a = (k-1)/2, b = k-1-a
-      for (int k = 1; k <= n; ++k) {
-        const int aa = (k - 1) >> 1, bb = k - 1 - aa;
-        cplx t = mkc(0.0, 0.0);
-        if (lane < rows) t = cmul(ld_c(Y + ((lane ^ 1) * (h + 1) + aa) * 2), ld_c(Y + (lane * (h + 1) + bb) * 2));
-        t = warp_sum_c(t);
-        if (lane == 0) st_c(acc_v + 2 * k, cadd(ld_c(acc_v + 2 * k), cscale(t, 0.5)));
-      }
-    }
-    __syncwarp();
+  switch ((2 * s + 7) >> 3) {
+#define GBSB_HP(NT, MS) \
+  haf_powers<NT, MS, CERT>(Cs, P, Y, Dv, acc_p, Ca, M, Ym, bT, s, cs, ps, n, h, loop, lane); break;
+    case 1: GBSB_HP(1, 1)
+    case 2: GBSB_HP(2, 1)
+    case 3: GBSB_HP(3, 1)
+    case 4: GBSB_HP(4, 1)
+    case 5: GBSB_HP(5, 2)
+    case 6: GBSB_HP(6, 2)
+    case 7: GBSB_HP(7, 2)
+    default: GBSB_HP(8, 2)
+#undef GBSB_HP
   }
+  __syncwarp();
 
-  // ---- Newton recurrence, every lane redundantly (identical values)
-  if (lane == 0) {
+  if (loop) {
+    // v_k = 1/2 sum_i y_a[i^1] y_b[i],  a = (k-1)/2, b = k-1-a
     for (int k = 1; k <= n; ++k) {
-      cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
-      if (loop) g = cadd(g, cscale(ld_c(acc_v + 2 * k), (double)k));
-      st_c(kg + 2 * k, g);
+      const int aa = (k - 1) >> 1, bb = k - 1 - aa;
+      cplx t = mkc(0.0, 0.0);
+      if (lane < s) t = cmul(ld_c(Y + ((lane ^ 1) * hp1 + aa) * 2), ld_c(Y + (lane * hp1 + bb) * 2));
+      t = warp_sum_c(t);
+      if (lane == 0) st_c(acc_v + 2 * k, cscale(t, 0.5));
+      if constexpr (CERT) {
+        double vb = lane < s ? ru_mul(Ym[(lane ^ 1) * hp1 + aa], Ym[lane * hp1 + bb]) : 0.0;
+        vb = warp_sum_ru(vb);
+        if (lane == 0) bV[k] = vb;
+      }
     }
-    st_c(ev, mkc(1.0, 0.0));
-    for (int j = 1; j <= n; ++j) {
-      cplx acc = mkc(0.0, 0.0);
-      for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(ld_c(kg + 2 * k), ld_c(ev + 2 * (j - k))));
-      st_c(ev + 2 * j, mkc(acc.re / j, acc.im / j));
+    __syncwarp();
+  }
+
+  // ---- Newton recurrence (lane 0), then broadcast through shared memory
+  double* eb = bT;  // reused after the bounds are folded into kg (certified tier)
+  if (lane == 0) {
+    if constexpr (CERT) {
+      // value-path coefficients: E_a <= c_a M_a with M_a = |C|^a, M_a <= phi_a M^_a
+      const double g2s = gamma_ru((double)(2 * s), 2.0 * kU);  // FP64 MMA, faithful rounding
+      const double sq2 = 1.4142135623730952;
+      const double g64 = ru_mul(sq2, gamma_ru(64.0, kU));
+      const double gy = ru_mul(sq2, gamma_ru((double)(s + 4), kU));
+      const double gv = ru_add(4.0 * kU, gamma_ru(8.0, kU));
+      double ca[kHafMaxPow + 2], ph[kHafMaxPow + 2], ka[kHafMaxPow + 2];
+      ca[0] = 0.0; ph[0] = 1.0; ca[1] = 0.0; ph[1] = 1.0;
+      for (int a = 1; a <= h; ++a) {
+        ca[a + 1] = ru_add(ca[a], ru_mul(ru_mul(sq2, g2s), ru_add(1.0, ca[a])));
+        ph[a + 1] = ru_div(ph[a], rd_sub(1.0, g2s));
+      }
+      ka[0] = 0.0;
+      for (int a = 1; a <= h; ++a) ka[a] = ru_add(ca[a], ru_mul(gy, ru_add(1.0, ca[a])));
+      cball kgb[kHafMaxPairs + 1];
+      for (int k = 1; k <= n; ++k) {
+        double ep;
+        if (k == 1) {
+          ep = ru_mul(gamma_ru(6.0, kU), bT[1]);
+        } else if ((k & 1) == 0) {
+          const int a = k / 2;
+          double f = ru_add(ru_add(ru_mul(2.0, ca[a]), ru_mul(ca[a], ca[a])),
+                            ru_mul(g64, ru_mul(ru_add(1.0, ca[a]), ru_add(1.0, ca[a]))));
+          ep = ru_mul(ru_mul(f, ru_mul(ph[a], ph[a])), bT[k]);
+        } else {
+          const int a = (k + 1) / 2;
+          double f = ru_add(ru_add(ru_add(ca[a], ca[a - 1]), ru_mul(ca[a], ca[a - 1])),
+                            ru_mul(g64, ru_mul(ru_add(1.0, ca[a]), ru_add(1.0, ca[a - 1]))));
+          ep = ru_mul(ru_mul(f, ru_mul(ph[a], ph[a - 1])), bT[k]);
+        }
+        cball g{cscale(ld_c(acc_p + 2 * k), 0.5), ru_mul(0.5, ep)};
+        if (loop) {
+          const int aa = (k - 1) >> 1, bb = k - 1 - aa;
+          double f = ru_add(ru_add(ru_add(ka[aa], ka[bb]), ru_mul(ka[aa], ka[bb])),
+                            ru_mul(gv, ru_mul(ru_add(1.0, ka[aa]), ru_add(1.0, ka[bb]))));
+          double evb = ru_mul(0.5, ru_mul(ru_mul(f, ru_mul(ph[aa], ph[bb])), bV[k]));
+          g = cb_add(g, cb_scale(cball{ld_c(acc_v + 2 * k), evb}, (double)k));
+        }
+        kgb[k] = g;
+      }
+      cball e[kHafMaxPairs + 1];
+      e[0] = cball{mkc(1.0, 0.0), 0.0};
+      for (int j = 1; j <= n; ++j) {
+        cball acc{mkc(0.0, 0.0), 0.0};
+        for (int k = 1; k <= j; ++k) acc = cb_add(acc, cb_mul(kgb[k], e[j - k]));
+        e[j] = cb_div_int(acc, (double)j);
+      }
+      st_c(ev + 2 * n, e[n].z);
+      eb[0] = e[n].r;
+    } else {
+      for (int k = 1; k <= n; ++k) {
+        cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
+        if (loop) g = cadd(g, cscale(ld_c(acc_v + 2 * k), (double)k));
+        st_c(kg + 2 * k, g);
+      }
+      st_c(ev, mkc(1.0, 0.0));
+      for (int j = 1; j <= n; ++j) {
+        cplx acc = mkc(0.0, 0.0);
+        for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(ld_c(kg + 2 * k), ld_c(ev + 2 * (j - k))));
+        st_c(ev + 2 * j, mkc(acc.re / j, acc.im / j));
+      }
     }
   }
   __syncwarp();
   cplx coeff = ld_c(ev + 2 * n);
+  double rad = 0.0;
+  if constexpr (CERT) rad = eb[0];
   __syncwarp();
-  return ((n - m) & 1) ? cneg(coeff) : coeff;
+  return cball{((n - m) & 1) ? cneg(coeff) : coeff, rad};
 }
 
 }  // namespace gbsb

@@ -43,6 +43,8 @@ GBSB_DECL_GROUP(haf)
 GBSB_DECL_GROUP(haf_dd)
 GBSB_DECL_GROUP(tor)
 GBSB_DECL_GROUP(mixed)
+GBSB_DECL_GROUP(perm_cert)
+GBSB_DECL_GROUP(cert)
 #undef GBSB_DECL_GROUP
 
 static cudaError_t launch_any(unsigned br, const ItemLaunch& P, int grid, int warps, cudaStream_t s) {
@@ -54,6 +56,8 @@ static cudaError_t launch_any(unsigned br, const ItemLaunch& P, int grid, int wa
   if (items_launch_haf_dd(br, P, grid, warps, s, &e)) return e;
   if (items_launch_tor(br, P, grid, warps, s, &e)) return e;
   if (items_launch_mixed(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_perm_cert(br, P, grid, warps, s, &e)) return e;
+  if (items_launch_cert(br, P, grid, warps, s, &e)) return e;
   return cudaErrorInvalidValue;
 }
 static int occ_any(unsigned br, const ItemLaunch& P, int warps) {
@@ -65,6 +69,8 @@ static int occ_any(unsigned br, const ItemLaunch& P, int warps) {
   if ((r = items_occ_haf_dd(br, P, warps)) >= 0) return r;
   if ((r = items_occ_tor(br, P, warps)) >= 0) return r;
   if ((r = items_occ_mixed(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_perm_cert(br, P, warps)) >= 0) return r;
+  if ((r = items_occ_cert(br, P, warps)) >= 0) return r;
   return 0;
 }
 // Smallest compiled branch set covering `need`.
@@ -171,7 +177,8 @@ static int ws_for_plan(const Plan& P) {
     int w = 0;
     if (fn == kFnPerm) w = 2 * d.dim * d.dim;
     else if (fn == kFnTor) w = d.dim * d.dim;
-    else w = tier == kTierDD ? haf_dd_layout(P.haf_smax).total : haf_layout(P.haf_smax).total;
+    else if (tier == kTierDD) w = haf_dd_layout(P.haf_smax).total;
+    else w = haf_layout(P.haf_smax, tier == kTierCert).total;
     ws = std::max(ws, w);
   }
   return (ws + 3) & ~3;  // 32-byte multiple per warp
@@ -257,7 +264,7 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
   *trivial = false;
   *real_in = false;
   if (r.dim < 0) return fail(cudaErrorInvalidValue, "negative matrix dimension");
-  if (r.tier < 0 || r.tier > 2) return fail(cudaErrorInvalidValue, "unsupported precision tier");
+  if (r.tier < 0 || r.tier > 3) return fail(cudaErrorInvalidValue, "unsupported precision tier");
   switch (r.fn) {
     case kFnPerm:
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
@@ -340,7 +347,7 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
       groups[g].push_back(i);
     }
   } else {
-    groups.resize(4);
+    groups.resize(5);
     for (int i = 0; i < B; ++i) {
       if (s->plan_trivial[i]) continue;
       groups[reqs[i].fn == kFnPerm ? 1 + reqs[i].tier : 0].push_back(i);
@@ -455,8 +462,10 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
     L.ws_doubles = P.ws_doubles;
     L.haf_smax = P.haf_smax;
     G.br = cover(P.need);
-    int warps = opt.warps;
+    // one-warp blocks when each warp needs a large shared workspace (the hafnian
+    // families) so the SM packs as many warps as shared memory allows
     const size_t smem_per_warp = (size_t)P.ws_doubles * sizeof(double);
+    int warps = smem_per_warp >= 8192 ? 1 : opt.warps;
     while (warps > 1 && (size_t)warps * smem_per_warp > 200 * 1024) warps >>= 1;
     const int bps = occ_any(G.br, L, warps);
     if (bps <= 0) return fail(cudaErrorInvalidConfiguration, "work item kernel does not fit on an SM");
@@ -688,6 +697,22 @@ int gbs_perm_kappa_host(const double* m, int n, int b, double* o, double* a) { r
 int gbs_haf_kappa_host(const double* m, int N, int b, double* o, double* a) { return one_shot(kFnHaf, kTierKappa, m, N, b, o, a); }
 int gbs_lhaf_kappa_host(const double* m, int N, int b, double* o, double* a) { return one_shot(kFnLhaf, kTierKappa, m, N, b, o, a); }
 int gbs_tor_kappa_host(const double* m, int n, int b, double* o, double* a) { return one_shot(kFnTor, kTierKappa, m, 2 * n, b, o, a); }
+
+// ---- certified tier: value + rigorous bound (core/host_api.cu:248-262) ---------
+static int one_shot_cert(int fn, const double* m, int dim, int b, double* o, double* bound) {
+  if (b > 0 && !bound) return fail(cudaErrorInvalidValue, "null bound buffer");
+  for (size_t i = 0; i < 2ull * (size_t)dim * dim * (size_t)std::max(b, 0); ++i)
+    if (!std::isfinite(m[i])) return fail(cudaErrorInvalidValue, "certified evaluation requires finite input");
+  int rc = one_shot(fn, kTierCert, m, dim, b, o, bound);
+  if (rc == 0)
+    for (int i = 0; i < b; ++i)
+      if (std::isnan(o[2 * i])) bound[i] = INFINITY;
+  return rc;
+}
+int gbs_perm_certified_host(const double* m, int n, int b, double* o, double* e) { return one_shot_cert(kFnPerm, m, n, b, o, e); }
+int gbs_haf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnHaf, m, N, b, o, e); }
+int gbs_lhaf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnLhaf, m, N, b, o, e); }
+int gbs_tor_certified_host(const double* m, int n, int b, double* o, double* e) { return one_shot_cert(kFnTor, m, 2 * n, b, o, e); }
 
 // ---- auto tier on the device (gbskernels/__init__.py:272-297) ----------------
 // func: 0 perm, 1 haf, 2 lhaf, 3 tor; dim = matrix side.  tier_out: 0 fp64, 1 dd.

@@ -50,6 +50,15 @@ int gbs_haf_kappa_host(const double* mats, int N, int batch, double* out, double
 int gbs_lhaf_kappa_host(const double* mats, int N, int batch, double* out, double* absnorm);
 int gbs_tor_kappa_host(const double* mats, int n, int batch, double* out, double* absnorm);
 
+/* ---- certified tier: fp64 value (bit-identical to the fp64 tier) + a rigorous
+ * bound |value - exact| <= bound, carried in directed rounding.  Uncertifiable or
+ * off-domain elements return NaN with bound +inf; non-finite input is rejected.
+ * reference: core/host_api.cu:248-262 (gbs_*_certified_host)                     */
+int gbs_perm_certified_host(const double* mats, int n, int batch, double* out, double* bound);
+int gbs_haf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
+int gbs_lhaf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
+int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, double* bound);
+
 /* ---- auto tier on the device ----------------------------------------------
  * reference: gbskernels/__init__.py:272-297 (_gpu_auto_batched) whose fp64 pass is
  * gbs_*_kappa_host and whose rerun is gbs_*_dd_host; here both run in the library.
@@ -77,8 +86,8 @@ int gbs_dev_free(double* d_result);
  * size bucket).  mode 0: ONE persistent launch over a device work queue holding
  * every instance (functions, sizes and tiers mixed); mode 1: one launch per
  * (function, tier, size) bucket.  offsets[i] is in complex elements into `mats`.
- * tiers[i]: 0 fp64, 1 dd, 2 fp64 + sum|term| (aux[i]).  status[i]: 0 ok,
- * 1 torontonian off the physical domain.                                         */
+ * tiers[i]: 0 fp64, 1 dd, 2 fp64 + sum|term| (aux[i]), 3 certified (aux[i] = bound).
+ * status[i]: 0 ok, 1 torontonian off the physical domain, 2 uncertifiable.       */
 int gbs_queue_evaluate(gbs_session* s, int batch, const int* funcs, const int* tiers, const int* dims,
                        const long long* offsets, const double* mats, int mode, double* out, double* aux,
                        int* status);
