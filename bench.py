@@ -385,7 +385,7 @@ def main():
 
     # ---- serving loop: p50 / p99 latency beside throughput
     if not a.no_serving and hasattr(G, "serve_stream") and dist.world == 1:
-        line["serving"] = G.serve_stream(rate=3e4, n_req=4000, seed=5, offline_rate=value)
+        line["serving"] = G.serve_stream(rate=None, rate_frac=0.75, n_req=2000, seed=5)
 
     if dist.rank == 0:
         print(json.dumps(line), flush=True)

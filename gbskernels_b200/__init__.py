@@ -31,12 +31,12 @@ __version__ = "0.1.0"
 __all__ = [
     "perm", "perm_batched", "haf", "haf_batched", "lhaf", "lhaf_batched",
     "tor", "tor_batched", "tor_single", "gpu_available", "gpu_backend_kind",
-    "Workspace", "PRECISIONS", "queue_evaluate",
+    "Workspace", "PRECISIONS", "queue_evaluate", "Server", "serve_stream",
 ]
 
 PRECISIONS = ("fp64", "ref", "dd", "auto", "certified")
 _FN = {"perm": 0, "haf": 1, "lhaf": 2, "tor": 3}
-_TIER = {"fp64": 0, "dd": 1, "kappa": 2}
+_TIER = {"fp64": 0, "dd": 1, "kappa": 2, "certified": 3}
 _AUTO_KAPPA_MAX = 1e8  # gbskernels/__init__.py:240
 
 # Largest input side each kernel family supports (tor: 2n).
@@ -572,3 +572,6 @@ def queue_evaluate(funcs: list[str], mats: list[np.ndarray], precisions: list[st
     precisions = precisions or ["fp64"] * len(mats)
     with Workspace(persistent=persistent) as ws:
         return ws.evaluate(funcs, [np.asarray(m, dtype=np.complex128) for m in mats], precisions)
+
+
+from .serving import Server, serve_stream  # noqa: E402

@@ -22,7 +22,9 @@ BUILD = HERE / "_build"
 LIB = HERE / "libgbs_b200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+# -fmad=false: every fused multiply-add is an explicit fma() in the source, so the
+# rounding of a value does not depend on the kernel it is inlined into.
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
            "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 

@@ -86,7 +86,7 @@ __device__ ItemResult perm_item(const double* __restrict__ mats, const InstDesc&
 }
 
 template <int TIER>
-__device__ ItemResult haf_item(const double* __restrict__ mats, const InstDesc& d, const WorkItem& w,
+__device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, const InstDesc& d, const WorkItem& w,
                                bool loop, double* ws, int haf_smax, int lane) {
   ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStOk};
   const int N = d.dim, n = N / 2;

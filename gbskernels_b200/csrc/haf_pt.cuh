@@ -84,8 +84,8 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
 // layout: D[ms][nt][0..3] = rows (16ms+g, 16ms+g+8), complex column 4nt+t4 (re, im).
 template <int NT, int MS>
 __device__ __forceinline__ void power_product(const double* __restrict__ P, const double* __restrict__ Cs, int s,
-                                              int cs, int ps, int lane, double (&D)[MS][NT][4]) {
-  constexpr int KS2 = (NT * MS < 8) ? 2 : 1;  // split K when few tiles are in flight
+                                              int cs, int ps, int ntn, int lane, double (&D)[MS][NT][4]) {
+  constexpr int KS2 = (MS == 1) ? 2 : 1;  // one strip: split K so eight mma chains are in flight
   const int g = lane >> 2, t4 = lane & 3;
   double acc[KS2][MS][NT][4];
 #pragma unroll
@@ -111,9 +111,11 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
     const double* bp = bptr + ks * 4 * cs;
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-      const double b = __longlong_as_double(__double_as_longlong(bp[nt * 8]) ^ sgn);
+      if (nt < ntn) {
+        const double b = __longlong_as_double(__double_as_longlong(bp[nt * 8]) ^ sgn);
 #pragma unroll
-      for (int ms = 0; ms < MS; ++ms) dmma_m16n8k4(acc[k2][ms][nt], a0[ms], a1[ms], b);
+        for (int ms = 0; ms < MS; ++ms) dmma_m16n8k4(acc[k2][ms][nt], a0[ms], a1[ms], b);
+      }
     }
   };
   if constexpr (KS2 == 2) {
@@ -129,9 +131,9 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
 #pragma unroll
       for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) D[ms][nt][q] = acc[0][ms][nt][q] + acc[KS2 - 1][ms][nt][q];
+        for (int q = 0; q < 4; ++q) D[ms][nt][q] = __dadd_rn(acc[0][ms][nt][q], acc[KS2 - 1][ms][nt][q]);
   } else {
-#pragma unroll 2
+#pragma unroll 1
     for (int ks = 0; ks < ksn; ++ks) slice(ks, 0);
 #pragma unroll
     for (int ms = 0; ms < MS; ++ms)
@@ -307,9 +309,10 @@ __device__ __forceinline__ void rows_bound(const double (&D)[MS][NT][4], const d
 // real columns, MS strips of 16 rows).  Accumulates the traces into acc_p[k], the
 // loop vectors into Y and (certified) the trace / row bound sums into bT / Ym.
 template <int NT, int MS, bool CERT>
-__device__ __forceinline__ void haf_powers(const double* Cs, double* P, double* Y, const double* Dv, double* acc_p,
-                                           const double* Ca, double* M, double* Ym, double* bT, int s, int cs, int ps,
-                                           int n, int h, bool loop, int lane) {
+__device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, const double* Dv, double* acc_p,
+                                        const double* Ca, double* M, double* Ym, double* bT, int s, int cs, int ps,
+                                        int n, int h, bool loop, int lane) {
+  const int ntn = (2 * s + 7) >> 3;  // column tiles in use (<= NT)
   const int hp1 = h + 1;
   double D[MS][NT][4];
   // power 1 (P = C): p_2 and y_1
@@ -327,7 +330,7 @@ __device__ __forceinline__ void haf_powers(const double* Cs, double* P, double* 
     if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, 1, hp1, s, lane);
   }
   for (int a = 2; a <= h; ++a) {
-    power_product<NT, MS>(P, Cs, s, cs, ps, lane, D);
+    power_product<NT, MS>(P, Cs, s, cs, ps, ntn, lane, D);
     cplx to = warp_sum_c(odd_partial<NT, MS>(D, P, ps, s, lane));
     cplx te = warp_sum_c(even_partial<NT, MS>(D));
     if (lane == 0) {
@@ -339,7 +342,7 @@ __device__ __forceinline__ void haf_powers(const double* Cs, double* P, double* 
     if (loop) rows_times_d<NT, MS>(D, Dv, Y, a, hp1, s, lane);
     if constexpr (CERT) {
       double Dm[MS][NT][4];
-      power_product<NT, MS>(M, Ca, s, cs, ps, lane, Dm);
+      power_product<NT, MS>(M, Ca, s, cs, ps, ntn, lane, Dm);
       double bo = warp_sum_ru(odd_bound<NT, MS>(Dm, M, ps, s, lane));
       double be = warp_sum_ru(even_bound<NT, MS>(Dm));
       if (lane == 0) {
@@ -432,19 +435,12 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   }
   __syncwarp();
 
-  switch ((2 * s + 7) >> 3) {
-#define GBSB_HP(NT, MS) \
-  haf_powers<NT, MS, CERT>(Cs, P, Y, Dv, acc_p, Ca, M, Ym, bT, s, cs, ps, n, h, loop, lane); break;
-    case 1: GBSB_HP(1, 1)
-    case 2: GBSB_HP(2, 1)
-    case 3: GBSB_HP(3, 1)
-    case 4: GBSB_HP(4, 1)
-    case 5: GBSB_HP(5, 2)
-    case 6: GBSB_HP(6, 2)
-    case 7: GBSB_HP(7, 2)
-    default: GBSB_HP(8, 2)
-#undef GBSB_HP
-  }
+  // two tile shapes: one 16-row strip with up to 4 column tiles (s <= 16), two
+  // strips with up to 8 (s <= 32); unused tiles are skipped at run time.  Few
+  // shapes keep the instruction footprint small: every subset size runs one of
+  // two code paths.
+  if (s <= 16) haf_powers<4, 1, CERT>(Cs, P, Y, Dv, acc_p, Ca, M, Ym, bT, s, cs, ps, n, h, loop, lane);
+  else haf_powers<8, 2, CERT>(Cs, P, Y, Dv, acc_p, Ca, M, Ym, bT, s, cs, ps, n, h, loop, lane);
   __syncwarp();
 
   if (loop) {

@@ -91,8 +91,25 @@ constexpr int kTorCapModes = 24;
 struct Req {
   int fn, tier;
   int dim;              // matrix side as given by the caller (tor: 2n)
-  const double* mat;    // complex interleaved, row-major
+  const double* mat;    // complex interleaved, row-major (host); null for a state request
+  // resident-state request: the matrix is gathered on the device as
+  // state[idx[r]][idx[c]] (loop weights gamma[idx[r]] on the diagonal when gamma)
+  const double* state = nullptr;  // device, M x M complex
+  const double* gamma = nullptr;  // device, M complex (or null)
+  const int* idx = nullptr;       // host, dim indices
+  int M = 0;
+  int state_real = 0;
 };
+
+// Device gather of resident-state submatrices (k_gather.cu).
+struct GatherDesc {
+  long long out_off;   // doubles into the packed matrix buffer
+  long long idx_off;   // ints into the index array
+  const double* state;
+  const double* gamma;
+  int d, de, M, use_gamma;
+};
+cudaError_t launch_gather(const GatherDesc* descs, int n, const int* idx, double* mats, cudaStream_t st);
 
 struct Plan {
   std::vector<InstDesc> insts;
@@ -202,6 +219,10 @@ struct gbs_session {
   int sms = 148;
   gbsb::DevBuf mats, meta, part, paux, pst, done, head, out, aux, st;
   gbsb::PinBuf pin_in, pin_meta, pin_out;
+  gbsb::DevBuf gather;
+  gbsb::PinBuf pin_gather;
+  std::vector<gbsb::GatherDesc> gdesc;
+  std::vector<int> gidx;
   size_t reallocs = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_kernel_ms = 0.f;
@@ -289,9 +310,13 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
       if (r.dim / 2 > kTorCapModes) return fail(cudaErrorInvalidValue, "torontonian: modes above the cap 24");
       bool re = true;
-      const size_t nn = (size_t)r.dim * r.dim;
-      for (size_t i = 0; i < nn; ++i)
-        if (r.mat[2 * i + 1] != 0.0) { re = false; break; }
+      if (r.state) {
+        re = r.state_real != 0;
+      } else {
+        const size_t nn = (size_t)r.dim * r.dim;
+        for (size_t i = 0; i < nn; ++i)
+          if (r.mat[2 * i + 1] != 0.0) { re = false; break; }
+      }
       if (!re) return fail(cudaErrorNotSupported, "torontonian: complex O is not supported by the batched kernel");
       *real_in = true;
       *dim_eval = r.dim;
@@ -415,10 +440,19 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
   // ---- pack matrices (odd loop hafnians augmented by A (+) [1]) and upload once
   {
     double* dst = (double*)s->pin_in.p;
+    s->gdesc.clear();
+    s->gidx.clear();
     for (int i = 0; i < B; ++i) {
       if (s->plan_trivial[i]) continue;
       const long long o = off[i];
       const int d = reqs[i].dim, de = dim_eval[i];
+      if (reqs[i].state) {  // filled on the device by the gather kernel
+        GatherDesc gd{o, (long long)s->gidx.size(), reqs[i].state, reqs[i].gamma, d, de, reqs[i].M,
+                      reqs[i].gamma != nullptr};
+        s->gdesc.push_back(gd);
+        s->gidx.insert(s->gidx.end(), reqs[i].idx, reqs[i].idx + d);
+        continue;
+      }
       if (de == d) {
         std::memcpy(dst + o, reqs[i].mat, sizeof(double) * 2 * (size_t)d * d);
       } else {
@@ -431,6 +465,19 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
     if (mat_doubles > 0) {
       e = cudaMemcpyAsync(s->mats.p, s->pin_in.p, mat_doubles * sizeof(double), cudaMemcpyHostToDevice, s->stream);
       if (e != cudaSuccess) return fail(e, "uploading matrices");
+    }
+    if (!s->gdesc.empty()) {
+      const size_t gb = s->gdesc.size() * sizeof(GatherDesc), ib = s->gidx.size() * sizeof(int);
+      e = grow_pin(s->pin_gather, gb + ib + 64);
+      if (e == cudaSuccess) e = grow_dev(s->gather, gb + ib + 64, &s->reallocs);
+      if (e != cudaSuccess) return fail(e, "allocating gather descriptors");
+      std::memcpy(s->pin_gather.p, s->gdesc.data(), gb);
+      std::memcpy((char*)s->pin_gather.p + gb, s->gidx.data(), ib);
+      e = cudaMemcpyAsync(s->gather.p, s->pin_gather.p, gb + ib, cudaMemcpyHostToDevice, s->stream);
+      if (e == cudaSuccess)
+        e = launch_gather((const GatherDesc*)s->gather.p, (int)s->gdesc.size(),
+                          (const int*)((char*)s->gather.p + gb), (double*)s->mats.p, s->stream);
+      if (e != cudaSuccess) return fail(e, "gathering resident submatrices");
     }
   }
   // ---- queues
@@ -514,8 +561,8 @@ static int plan_launch(gbs_session* s, cudaStream_t stream) {
   return 0;
 }
 
-// Copy the plan's results back (synchronous) and scatter them to request order.
-static int plan_read(gbs_session* s, cudaStream_t stream, double* out, double* aux, int* st) {
+// Enqueue the device-to-host copies of the plan's results on `stream`.
+static int plan_read_enqueue(gbs_session* s, cudaStream_t stream) {
   if (!stream) stream = s->stream;
   const size_t ni = s->plan_ninst;
   double* po = (double*)s->pin_out.p;
@@ -527,11 +574,15 @@ static int plan_read(gbs_session* s, cudaStream_t stream, double* out, double* a
     if (e == cudaSuccess) e = cudaMemcpyAsync(pa, s->aux.p, ni * sizeof(double), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ps, s->st.p, ni * sizeof(int), cudaMemcpyDeviceToHost, stream);
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-  if (e != cudaSuccess) return fail(e, "evaluating the batch");
-  float ms = 0.f;
-  if (!s->groups.empty()) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-  s->last_kernel_ms = ms;
+  return e == cudaSuccess ? 0 : fail(e, "reading results back");
+}
+
+// Scatter the (already copied) results to request order.
+static void plan_collect(gbs_session* s, double* out, double* aux, int* st) {
+  const size_t ni = s->plan_ninst;
+  double* po = (double*)s->pin_out.p;
+  double* pa = po + 2 * ni;
+  int* ps = (int*)(pa + ni);
   for (const auto& G : s->groups)
     for (int k = 0; k < G.ni; ++k) {
       const int i = G.req[k];
@@ -548,6 +599,19 @@ static int plan_read(gbs_session* s, cudaStream_t stream, double* out, double* a
     if (aux) aux[i] = std::hypot(t.re, t.im);
     if (st) st[i] = kStOk;
   }
+}
+
+// Copy the plan's results back (synchronous) and scatter them to request order.
+static int plan_read(gbs_session* s, cudaStream_t stream, double* out, double* aux, int* st) {
+  if (!stream) stream = s->stream;
+  int rc = plan_read_enqueue(s, stream);
+  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(e, "evaluating the batch");
+  float ms = 0.f;
+  if (!s->groups.empty()) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  s->last_kernel_ms = ms;
+  plan_collect(s, out, aux, st);
   return 0;
 }
 
@@ -583,9 +647,10 @@ static int session_open(gbs_session** out) {
 static void session_free(gbs_session* s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
-  for (DevBuf* b : {&s->mats, &s->meta, &s->part, &s->paux, &s->pst, &s->done, &s->head, &s->out, &s->aux, &s->st})
+  for (DevBuf* b : {&s->mats, &s->meta, &s->part, &s->paux, &s->pst, &s->done, &s->head, &s->out, &s->aux, &s->st,
+                    &s->gather})
     if (b->p) cudaFree(b->p);
-  for (PinBuf* b : {&s->pin_in, &s->pin_meta, &s->pin_out})
+  for (PinBuf* b : {&s->pin_in, &s->pin_meta, &s->pin_out, &s->pin_gather})
     if (b->p) cudaFreeHost(b->p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -851,6 +916,395 @@ int gbs_session_last_stats(const gbs_session* s, double* kernel_ms, int* launche
   if (kernel_ms) *kernel_ms = s->last_kernel_ms;
   if (launches) *launches = s->last_launches;
   if (items) *items = s->last_items;
+  return 0;
+}
+
+}  // extern "C"
+
+// ====================================================================== serving loop
+// Continuous batching for chain-rule sampler queries (new; the reference serves no
+// requests -- its resident sampler session, core/sampler_session.cu:68-128, runs a
+// fixed chain).  A scheduler thread owns `slots` sessions (one stream each):
+//   1. a finished slot (its completion event has fired) delivers its results --
+//      an "auto" request whose indicator reaches kappa_max goes back to the front of
+//      the queue as a double-double request with the same ticket;
+//   2. a free slot admits the oldest pending requests up to the workspace budget
+//      (matrix bytes + per-item partials) and launches them as ONE persistent queue;
+//   3. with nothing to do it waits on the submission condition variable (bounded).
+// Requests that arrive while batches are on the GPU join the next free slot, so
+// up to `slots` batches overlap on the device.  A value never depends on its batch
+// (work items are a function of the request alone).
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+namespace gbsb {
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct SrvReq {
+  long long ticket = 0;
+  int fn = 0, tier = 0, dim = 0;
+  bool is_auto = false;
+  std::vector<double> mat;
+  int state = -1;
+  std::vector<int> idx;
+  bool use_gamma = false;
+  double t_submit = 0.0;
+};
+struct SrvRes {
+  double re = 0, im = 0, aux = 0;
+  int status = 0, tier_used = 0;
+  double t_submit = 0, t_done = 0;
+  bool done = false;
+};
+struct SrvState {
+  double* dA = nullptr;
+  double* dG = nullptr;
+  int M = 0;
+  int real = 0;
+};
+struct Slot {
+  gbs_session* s = nullptr;
+  bool busy = false;
+  std::vector<SrvReq> batch;
+  cudaEvent_t done = nullptr;
+};
+
+}  // namespace gbsb
+
+struct gbs_server {
+  std::vector<gbsb::Slot> slots;
+  std::vector<gbsb::SrvState> states;
+  std::deque<gbsb::SrvReq> pending;
+  std::unordered_map<long long, gbsb::SrvRes> results;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread worker;
+  bool stop = false;
+  int error = 0;
+  std::string error_msg;
+  long long next_ticket = 1;
+  size_t budget = 0;
+  int max_batch = 0;
+  double kappa_max = 1e8;
+  long long batches = 0, completed = 0, in_flight = 0;
+  int device = 0;
+};
+
+namespace gbsb {
+
+static size_t req_bytes(const SrvReq& r) {
+  const size_t d = (size_t)r.dim + 1;
+  size_t items = 1;
+  if (r.fn == kFnHaf || r.fn == kFnLhaf) items = (size_t)1 << std::max(0, (int)(d / 2) - 9);
+  return d * d * 16 + items * 48 + 256;
+}
+
+static int srv_launch(gbs_server* sv, Slot& sl) {
+  std::vector<Req> reqs(sl.batch.size());
+  for (size_t i = 0; i < sl.batch.size(); ++i) {
+    const SrvReq& q = sl.batch[i];
+    Req r{q.fn, q.tier, q.dim, q.mat.empty() ? nullptr : q.mat.data()};
+    if (q.state >= 0) {
+      const SrvState& S = sv->states[q.state];
+      r.state = S.dA;
+      r.gamma = q.use_gamma ? S.dG : nullptr;
+      r.idx = q.idx.data();
+      r.M = S.M;
+      r.state_real = S.real;
+    }
+    reqs[i] = r;
+  }
+  RunOpts opt;
+  int rc = plan_build(sl.s, reqs, opt);
+  if (rc == 0) rc = plan_launch(sl.s, nullptr);
+  if (rc == 0) rc = plan_read_enqueue(sl.s, nullptr);
+  if (rc == 0) {
+    cudaError_t e = cudaEventRecord(sl.done, sl.s->stream);
+    if (e != cudaSuccess) rc = fail(e, "recording a completion event");
+  }
+  return rc;
+}
+
+static void srv_loop(gbs_server* sv) {
+  cudaSetDevice(sv->device);
+  std::unique_lock<std::mutex> lk(sv->mu);
+  for (;;) {
+    bool progressed = false;
+    // 1. completions
+    for (Slot& sl : sv->slots) {
+      if (!sl.busy) continue;
+      cudaError_t q = cudaEventQuery(sl.done);
+      if (q == cudaErrorNotReady) continue;
+      const size_t B = sl.batch.size();
+      std::vector<double> out(2 * B), aux(B);
+      std::vector<int> st(B);
+      if (q != cudaSuccess) {
+        sv->error = (int)q;
+        sv->error_msg = "serving batch failed";
+        for (size_t i = 0; i < B; ++i) st[i] = kStTimeout;
+      } else {
+        plan_collect(sl.s, out.data(), aux.data(), st.data());
+      }
+      const double t = now_s();
+      for (size_t i = 0; i < B; ++i) {
+        SrvReq& r = sl.batch[i];
+        if (r.is_auto && r.tier == kTierKappa && st[i] == kStOk) {
+          const double mag = std::max(std::hypot(out[2 * i], out[2 * i + 1]), 1e-300);
+          if (!(aux[i] / mag < sv->kappa_max)) {
+            SrvReq again = r;
+            again.tier = kTierDD;
+            sv->pending.push_front(std::move(again));
+            sv->results[r.ticket].aux = aux[i] / mag;
+            continue;
+          }
+        }
+        SrvRes& res = sv->results[r.ticket];
+        res.re = out[2 * i];
+        res.im = out[2 * i + 1];
+        if (st[i] != kStOk) { res.re = NAN; res.im = NAN; }
+        if (r.is_auto) {
+          if (r.tier == kTierKappa) res.aux = aux[i] / std::max(std::hypot(res.re, res.im), 1e-300);
+          res.tier_used = r.tier == kTierDD ? 1 : 0;
+        } else {
+          res.aux = (r.tier == kTierCert && st[i] != kStOk) ? INFINITY : aux[i];
+          res.tier_used = r.tier;
+        }
+        res.status = st[i];
+        res.t_done = t;
+        res.done = true;
+        ++sv->completed;
+      }
+      sv->in_flight -= (long long)B;
+      sl.batch.clear();
+      sl.busy = false;
+      progressed = true;
+    }
+    // 2. admission
+    for (Slot& sl : sv->slots) {
+      if (sl.busy || sv->pending.empty()) continue;
+      size_t bytes = 0;
+      while (!sv->pending.empty() && (int)sl.batch.size() < sv->max_batch) {
+        const size_t b = req_bytes(sv->pending.front());
+        if (!sl.batch.empty() && bytes + b > sv->budget) break;
+        bytes += b;
+        sl.batch.push_back(std::move(sv->pending.front()));
+        sv->pending.pop_front();
+      }
+      sv->in_flight += (long long)sl.batch.size();
+      lk.unlock();
+      int rc = srv_launch(sv, sl);
+      lk.lock();
+      if (rc) {
+        sv->error = rc;
+        sv->error_msg = g_last_error;
+        for (SrvReq& r : sl.batch) {
+          SrvRes& res = sv->results[r.ticket];
+          res.re = res.im = NAN;
+          res.status = kStTimeout;
+          res.done = true;
+          res.t_done = now_s();
+          ++sv->completed;
+        }
+        sv->in_flight -= (long long)sl.batch.size();
+        sl.batch.clear();
+      } else {
+        sl.busy = true;
+        ++sv->batches;
+      }
+      progressed = true;
+    }
+    bool any_busy = false;
+    for (Slot& sl : sv->slots) any_busy |= sl.busy;
+    if (sv->stop && sv->pending.empty() && !any_busy) break;
+    if (!progressed) {
+      if (any_busy) {
+        // poll the completion events at a fine granularity without holding the lock
+        lk.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        lk.lock();
+      } else {
+        sv->cv.wait_for(lk, std::chrono::milliseconds(2));
+      }
+    }
+  }
+}
+
+}  // namespace gbsb
+
+extern "C" {
+
+// Open a server with `n_slots` concurrent batches, a per-batch workspace budget in
+// bytes (admission control) and a per-batch request cap.
+int gbs_server_open(int n_slots, long long budget_bytes, int max_batch, gbs_server** out) {
+  if (!out || n_slots < 1 || n_slots > 64) return fail(cudaErrorInvalidValue, "bad server arguments");
+  gbs_server* sv = new gbs_server();
+  cudaGetDevice(&sv->device);
+  sv->budget = budget_bytes > 0 ? (size_t)budget_bytes : ((size_t)256 << 20);
+  sv->max_batch = max_batch > 0 ? max_batch : 4096;
+  sv->slots.resize(n_slots);
+  for (Slot& sl : sv->slots) {
+    int rc = session_open(&sl.s);
+    cudaError_t e = rc == 0 ? cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) : cudaErrorUnknown;
+    if (rc || e != cudaSuccess) {
+      for (Slot& t : sv->slots) {
+        if (t.s) session_free(t.s);
+        if (t.done) cudaEventDestroy(t.done);
+      }
+      delete sv;
+      return fail(rc ? rc : (int)e, "opening server slots");
+    }
+  }
+  sv->worker = std::thread(srv_loop, sv);
+  *out = sv;
+  return 0;
+}
+
+// Drain every pending request, stop the scheduler and free the slots.
+int gbs_server_close(gbs_server* sv) {
+  if (!sv) return 0;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv.notify_all();
+  if (sv->worker.joinable()) sv->worker.join();
+  for (Slot& sl : sv->slots) {
+    if (sl.s) session_free(sl.s);
+    if (sl.done) cudaEventDestroy(sl.done);
+  }
+  for (SrvState& st : sv->states) {
+    if (st.dA) cudaFree(st.dA);
+    if (st.dG) cudaFree(st.dG);
+  }
+  delete sv;
+  return 0;
+}
+
+// Upload a resident state: an M x M complex matrix (the GBS kernel A, or O in
+// xxpp for torontonians) and optional M loop weights.  Returns its id.
+int gbs_server_add_state(gbs_server* sv, const double* A, const double* gamma, int M, int* state_id) {
+  if (!sv || !A || M <= 0 || !state_id) return fail(cudaErrorInvalidValue, "bad state arguments");
+  SrvState S;
+  S.M = M;
+  S.real = 1;
+  for (size_t i = 0; i < (size_t)M * M; ++i)
+    if (A[2 * i + 1] != 0.0) { S.real = 0; break; }
+  cudaError_t e = cudaMalloc(&S.dA, (size_t)M * M * 16);
+  if (e == cudaSuccess) e = cudaMemcpy(S.dA, A, (size_t)M * M * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && gamma) {
+    e = cudaMalloc(&S.dG, (size_t)M * 16);
+    if (e == cudaSuccess) e = cudaMemcpy(S.dG, gamma, (size_t)M * 16, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    if (S.dA) cudaFree(S.dA);
+    if (S.dG) cudaFree(S.dG);
+    return fail(e, "uploading a resident state");
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->states.push_back(S);
+  *state_id = (int)sv->states.size() - 1;
+  return 0;
+}
+
+static int srv_submit(gbs_server* sv, gbsb::SrvReq&& r, long long* ticket) {
+  if (r.tier < 0 || r.tier > 3) return fail(cudaErrorInvalidValue, "tier must be 0 fp64, 1 dd, 2 auto, 3 certified");
+  if (r.tier == 2) { r.is_auto = true; r.tier = kTierKappa; }
+  r.t_submit = now_s();
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->stop) return fail(cudaErrorInvalidValue, "server is closing");
+    r.ticket = sv->next_ticket++;
+    SrvRes& res = sv->results[r.ticket];
+    res.t_submit = r.t_submit;
+    *ticket = r.ticket;
+    sv->pending.push_back(std::move(r));
+  }
+  sv->cv.notify_one();
+  return 0;
+}
+
+// Submit one request with an explicit matrix (dim x dim complex; tor: 2n x 2n).
+// tier: 0 fp64, 1 dd, 2 auto (fp64 + indicator, double-double rerun), 3 certified.
+int gbs_server_submit(gbs_server* sv, int func, int tier, int dim, const double* mat, long long* ticket) {
+  if (!sv || !ticket || dim < 0 || (dim > 0 && !mat)) return fail(cudaErrorInvalidValue, "bad request");
+  gbsb::SrvReq r;
+  r.fn = func;
+  r.tier = tier;
+  r.dim = dim;
+  r.mat.assign(mat, mat + 2 * (size_t)dim * dim);
+  return srv_submit(sv, std::move(r), ticket);
+}
+
+// Submit one request on a resident state: the matrix is state[idx][:, idx]
+// (use_gamma: the state's loop weights on the diagonal), gathered on the device.
+int gbs_server_submit_state(gbs_server* sv, int func, int tier, int state, int n_idx, const int* idx, int use_gamma,
+                            long long* ticket) {
+  if (!sv || !ticket || n_idx < 0 || (n_idx > 0 && !idx)) return fail(cudaErrorInvalidValue, "bad request");
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (state < 0 || state >= (int)sv->states.size()) return fail(cudaErrorInvalidValue, "unknown state");
+    for (int i = 0; i < n_idx; ++i)
+      if (idx[i] < 0 || idx[i] >= sv->states[state].M) return fail(cudaErrorInvalidValue, "index outside the state");
+    if (use_gamma && !sv->states[state].dG) return fail(cudaErrorInvalidValue, "state has no loop weights");
+  }
+  gbsb::SrvReq r;
+  r.fn = func;
+  r.tier = tier;
+  r.dim = n_idx;
+  r.state = state;
+  r.idx.assign(idx, idx + n_idx);
+  r.use_gamma = use_gamma != 0;
+  return srv_submit(sv, std::move(r), ticket);
+}
+
+// Non-blocking poll.  When done: out = value (complex), aux = kappa (auto) or bound
+// (certified), tier_used (0 fp64, 1 dd, 3 certified), latency_s = completion -
+// submission; the result is then released.
+int gbs_server_poll(gbs_server* sv, long long ticket, int* done, double* out, double* aux, int* status,
+                    int* tier_used, double* latency_s) {
+  if (!sv || !done) return fail(cudaErrorInvalidValue, "null argument");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->results.find(ticket);
+  if (it == sv->results.end()) return fail(cudaErrorInvalidValue, "unknown ticket");
+  *done = it->second.done ? 1 : 0;
+  if (!it->second.done) return 0;
+  const SrvRes& r = it->second;
+  if (out) { out[0] = r.re; out[1] = r.im; }
+  if (aux) *aux = r.aux;
+  if (status) *status = r.status;
+  if (tier_used) *tier_used = r.tier_used;
+  if (latency_s) *latency_s = r.t_done - r.t_submit;
+  sv->results.erase(it);
+  return 0;
+}
+
+// Wait (bounded) until nothing is pending or in flight.  Returns 0, or
+// cudaErrorTimeout when `timeout_s` elapsed first.
+int gbs_server_drain(gbs_server* sv, double timeout_s) {
+  if (!sv) return fail(cudaErrorInvalidValue, "null server");
+  const double t0 = now_s();
+  for (;;) {
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      if (sv->pending.empty() && sv->in_flight == 0) return sv->error ? fail(sv->error, sv->error_msg) : 0;
+    }
+    if (now_s() - t0 > timeout_s) return fail(cudaErrorTimeout, "server drain timed out");
+    std::this_thread::sleep_for(std::chrono::microseconds(200));
+  }
+}
+
+int gbs_server_stats(gbs_server* sv, long long* completed, long long* batches, long long* pending) {
+  if (!sv) return fail(cudaErrorInvalidValue, "null server");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (completed) *completed = sv->completed;
+  if (batches) *batches = sv->batches;
+  if (pending) *pending = (long long)sv->pending.size() + sv->in_flight;
   return 0;
 }
 

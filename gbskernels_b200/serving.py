@@ -1,0 +1,198 @@
+"""Continuous-batching server for chain-rule sampler queries (libgbs_b200 gbs_server_*).
+
+    with Server(slots=4) as srv:
+        st = srv.add_state(A, gamma)                      # resident on the device
+        t = srv.submit_state("lhaf", st, idx, "auto", use_gamma=True)
+        value, diag = srv.result(t)                       # blocks (bounded) until done
+
+The scheduler runs in the library (a C++ thread): requests that arrive while
+batches are on the GPU are admitted into the next free slot, up to a workspace
+budget per batch, and up to `slots` batches overlap on the device.  A value is
+independent of the batch it ran in.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .workloads import serving_stream
+
+_FN = {"perm": 0, "haf": 1, "lhaf": 2, "tor": 3}
+_TIER = {"fp64": 0, "dd": 1, "auto": 2, "certified": 3}
+_TIER_NAME = {0: "fp64", 1: "dd", 3: "certified-fp64"}
+
+_vp = ctypes.c_void_p
+_SIGS = {
+    "gbs_server_open": ([ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "gbs_server_close": ([_vp], ctypes.c_int),
+    "gbs_server_add_state": ([_vp, _lib._dp, _lib._dp, ctypes.c_int, _lib._ip], ctypes.c_int),
+    "gbs_server_submit": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _lib._dp,
+                           ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "gbs_server_submit_state": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _lib._ip,
+                                 ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "gbs_server_poll": ([_vp, ctypes.c_longlong, _lib._ip, _lib._dp, _lib._dp, _lib._ip, _lib._ip, _lib._dp],
+                        ctypes.c_int),
+    "gbs_server_drain": ([_vp, ctypes.c_double], ctypes.c_int),
+    "gbs_server_stats": ([_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                          ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+}
+_lib.SIGNATURES.update(_SIGS)
+
+
+def _l():
+    lib = _lib.load()
+    for name, (a, r) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes, fn.restype = a, r
+    return lib
+
+
+class Server:
+    """Serving session: `slots` concurrent batches, `budget_bytes` per batch."""
+
+    def __init__(self, slots: int = 4, budget_bytes: int = 256 << 20, max_batch: int = 4096):
+        self._lib = _l()
+        h = _vp()
+        _lib.check(self._lib.gbs_server_open(slots, budget_bytes, max_batch, ctypes.byref(h)), "gbs_server_open")
+        self._h = h
+        self._keep: list = []
+
+    def __enter__(self) -> "Server":
+        return self
+
+    def __exit__(self, *exc) -> bool:
+        self.close()
+        return False
+
+    def close(self) -> None:
+        if self._h is not None:
+            self._lib.gbs_server_close(self._h)
+            self._h = None
+
+    def add_state(self, A, gamma=None) -> int:
+        A = np.ascontiguousarray(np.asarray(A, dtype=np.complex128))
+        if A.ndim != 2 or A.shape[0] != A.shape[1]:
+            raise ValueError("state must be a square matrix")
+        g = None if gamma is None else np.ascontiguousarray(np.asarray(gamma, dtype=np.complex128))
+        sid = np.zeros(1, dtype=np.int32)
+        _lib.check(self._lib.gbs_server_add_state(self._h, _lib.dptr(A.view(np.float64)),
+                                                  None if g is None else _lib.dptr(g.view(np.float64)),
+                                                  A.shape[0], _lib.iptr(sid)), "gbs_server_add_state")
+        return int(sid[0])
+
+    def submit(self, func: str, mat, precision: str = "fp64") -> int:
+        m = np.ascontiguousarray(np.asarray(mat, dtype=np.complex128))
+        t = ctypes.c_longlong()
+        _lib.check(self._lib.gbs_server_submit(self._h, _FN[func], _TIER[precision], m.shape[0],
+                                               _lib.dptr(m.view(np.float64)), ctypes.byref(t)),
+                   "gbs_server_submit")
+        return t.value
+
+    def submit_state(self, func: str, state: int, idx, precision: str = "fp64", use_gamma: bool = False) -> int:
+        ix = np.ascontiguousarray(np.asarray(idx, dtype=np.int32))
+        t = ctypes.c_longlong()
+        _lib.check(self._lib.gbs_server_submit_state(self._h, _FN[func], _TIER[precision], state, ix.size,
+                                                     _lib.iptr(ix), int(use_gamma), ctypes.byref(t)),
+                   "gbs_server_submit_state")
+        return t.value
+
+    def poll(self, ticket: int):
+        """(done, value, info) without blocking; info has tier, aux, status, latency_s."""
+        done = np.zeros(1, dtype=np.int32)
+        out = np.zeros(2)
+        aux = np.zeros(1)
+        st = np.zeros(1, dtype=np.int32)
+        tier = np.zeros(1, dtype=np.int32)
+        lat = np.zeros(1)
+        _lib.check(self._lib.gbs_server_poll(self._h, ticket, _lib.iptr(done), _lib.dptr(out), _lib.dptr(aux),
+                                             _lib.iptr(st), _lib.iptr(tier), _lib.dptr(lat)), "gbs_server_poll")
+        if not done[0]:
+            return False, None, None
+        info = {"tier": _TIER_NAME.get(int(tier[0]), str(int(tier[0]))), "aux": float(aux[0]),
+                "status": int(st[0]), "latency_s": float(lat[0])}
+        return True, complex(out[0], out[1]), info
+
+    def result(self, ticket: int, timeout_s: float = 120.0):
+        t0 = time.perf_counter()
+        while True:
+            done, v, info = self.poll(ticket)
+            if done:
+                return v, info
+            if time.perf_counter() - t0 > timeout_s:
+                raise TimeoutError(f"request {ticket} not done after {timeout_s} s")
+            time.sleep(50e-6)
+
+    def drain(self, timeout_s: float = 600.0) -> None:
+        _lib.check(self._lib.gbs_server_drain(self._h, timeout_s), "gbs_server_drain")
+
+    def stats(self) -> dict:
+        c, b, p = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.check(self._lib.gbs_server_stats(self._h, ctypes.byref(c), ctypes.byref(b), ctypes.byref(p)),
+                   "gbs_server_stats")
+        return {"completed": c.value, "batches": b.value, "pending": p.value}
+
+
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, rate_frac: float = 0.7,
+                 slots: int = 4, budget_bytes: int = 64 << 20):
+    """Replay a Poisson stream of chain-rule queries (haf / lhaf / tor, N 6..30,
+    fp64 70% / auto 20% / certified 10%) against a Server.
+
+    The offline rate of the same requests (one persistent mixed batch) is measured
+    first; the stream is offered at `rate` requests/s, or at rate_frac x the offline
+    rate when `rate` is None.  Returns throughput, p50/p99 latency, the offline rate
+    and the ratio throughput / offline rate."""
+    from . import Workspace
+
+    reqs0 = serving_stream(n_req, 1.0, seed=seed)
+    # offline: the same requests as one persistent mixed batch (auto -> its fp64 +
+    # indicator pass; the rare double-double reruns are not part of the offline rate)
+    tier_of = {"fp64": "fp64", "auto": "kappa", "certified": "certified"}
+    funcs = [r[1] for r in reqs0]
+    mats = [r[3] for r in reqs0]
+    tiers = [tier_of[r[2]] for r in reqs0]
+    with Workspace() as ws:
+        ws.evaluate(funcs[:64], mats[:64], tiers[:64])  # warm-up
+        t0 = time.perf_counter()
+        ws_out = ws.evaluate(funcs, mats, tiers)
+        t_off = time.perf_counter() - t0
+    off_rate = n_req / t_off
+    if rate is None:
+        rate = rate_frac * off_rate
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=n_req)
+    arrivals = np.cumsum(gaps)
+    reqs = [(float(arrivals[i]),) + tuple(reqs0[i][1:]) for i in range(n_req)]
+    lat = []
+    with Server(slots=slots, budget_bytes=budget_bytes) as srv:
+        # warm the slots
+        for r in reqs[:8]:
+            srv.result(srv.submit(r[1], r[3], r[2]))
+        tickets = []
+        t_start = time.perf_counter()
+        for (ta, func, prec, mat) in reqs:
+            while time.perf_counter() - t_start < ta:
+                pass
+            tickets.append(srv.submit(func, mat, prec))
+        vals = []
+        for t in tickets:
+            v, info = srv.result(t)
+            lat.append(info["latency_s"])
+            vals.append(v)
+        t_end = time.perf_counter()
+        stats = srv.stats()
+    thr = n_req / (t_end - t_start)
+    fp = [i for i, r in enumerate(reqs) if r[2] in ("fp64", "certified")]
+    same = bool(all(vals[i] == ws_out[i] or (np.isnan(vals[i]) and np.isnan(ws_out[i])) for i in fp))
+    return {"offered_rate": rate, "requests": n_req, "throughput": thr, "unit": "requests/s",
+            "p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99), "max_ms": 1e3 * max(lat),
+            "offline_rate": off_rate, "throughput_vs_offline": thr / off_rate,
+            "batches": stats["batches"], "slots": slots,
+            "values_equal_to_offline_batch": same}
+

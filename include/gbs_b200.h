@@ -101,6 +101,30 @@ int gbs_queue_read(gbs_session* s, void* stream, double* out, double* aux, int* 
 /* kernel time (CUDA events), launches and work items of the session's last call */
 int gbs_session_last_stats(const gbs_session* s, double* kernel_ms, int* launches, long long* items);
 
+/* ---- continuous-batching server (chain-rule sampler queries) -----------------
+ * No reference counterpart (the reference's resident sampler session,
+ * core/sampler_session.cu:68-128, runs one fixed chain; it serves no requests).
+ * A scheduler thread owns `n_slots` sessions (one stream each); requests that
+ * arrive while batches run are admitted into the next free slot up to
+ * `budget_bytes` of workspace per batch; up to n_slots batches overlap on the GPU.
+ * tier: 0 fp64, 1 dd, 2 auto (fp64 + indicator, device double-double rerun when
+ * kappa >= 1e8), 3 certified.  Resident states (M x M complex + optional M loop
+ * weights) stay in HBM; a state request's matrix state[idx][:, idx] is gathered on
+ * the device (core/sampler_gather.cu:20-57 is the reference's gather).           */
+typedef struct gbs_server gbs_server;
+int gbs_server_open(int n_slots, long long budget_bytes, int max_batch, gbs_server** out);
+int gbs_server_close(gbs_server* sv);
+int gbs_server_add_state(gbs_server* sv, const double* A, const double* gamma, int M, int* state_id);
+int gbs_server_submit(gbs_server* sv, int func, int tier, int dim, const double* mat, long long* ticket);
+int gbs_server_submit_state(gbs_server* sv, int func, int tier, int state, int n_idx, const int* idx,
+                            int use_gamma, long long* ticket);
+/* non-blocking; when *done: out[2] value, aux = kappa (auto) / bound (certified),
+ * tier_used 0 fp64 / 1 dd / 3 certified, latency_s = completion - submission      */
+int gbs_server_poll(gbs_server* sv, long long ticket, int* done, double* out, double* aux, int* status,
+                    int* tier_used, double* latency_s);
+int gbs_server_drain(gbs_server* sv, double timeout_s);
+int gbs_server_stats(gbs_server* sv, long long* completed, long long* batches, long long* pending);
+
 /* ---- measurement ------------------------------------------------------------
  * FP64 tensor-core throughput of this GPU (mma .m16n8k8 .f64 chains on every SM),
  * the denominator of the kernels' roofline fraction.  No reference counterpart.  */
