@@ -110,13 +110,24 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     r.aux = acc.r;
     if (!isfinite(acc.r) || !isfinite(acc.z.re) || !isfinite(acc.z.im)) r.st = kStUncertified;
   } else {
+    // the traces of kHafRing subsets are parked, then kHafRing lanes run their
+    // Newton recurrences at once (see haf_ring_flush)
     const HafLayout L = haf_layout(haf_smax);
+    double* ring = ws + L.ring_off;
     cplx acc = mkc(0.0, 0.0);
     double absacc = 0.0;
+    int cnt = 0;
     for (unsigned long long k = 0; k < w.count; ++k) {
-      cplx t = haf_subset_term_tc<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane).z;
-      acc = cadd(acc, t);
-      if (TIER == kTierKappa) absacc += cabs_fast(t);
+      haf_subset_term_tc<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane, ring + cnt * kHafRingSlot * 2);
+      if (++cnt == kHafRing || k + 1 == w.count) {
+        __syncwarp();
+        double ab = 0.0;
+        const cplx t = haf_ring_flush(ring, cnt, n, lane, TIER == kTierKappa ? &ab : nullptr);
+        acc = cadd(acc, t);
+        absacc += ab;
+        cnt = 0;
+        __syncwarp();
+      }
     }
     r.val = ddc_from_c(acc);
     r.aux = absacc;

@@ -46,9 +46,15 @@ __host__ __device__ inline int haf_p_stride(int s) { return (s % 4 == 2) ? s : s
 __host__ __device__ inline int haf_strips(int s) { return (s + 15) / 16; }
 
 // Per-warp shared-memory workspace (doubles), laid out for a launch-wide max s.
+// Batched Newton recurrence: the traces of kHafRing consecutive subsets are parked
+// in a ring (slot: kg[1..n] and the sign), then kHafRing lanes run one recurrence
+// each.  Slot k[0] holds (sign, 0) or (0, 0) for an empty subset.
+constexpr int kHafRing = 16;
+constexpr int kHafRingSlot = kHafMaxPairs + 1;  // complex entries per slot
+
 struct HafLayout {
   int smax;
-  int c_off, p_off, y_off, d_off, gi_off, acc_off, total;  // in doubles
+  int c_off, p_off, y_off, d_off, gi_off, acc_off, ring_off, total;  // in doubles
   // certified tier only: |C|, the bound-path power, row bounds and trace-bound sums
   int ca_off, m_off, ym_off, bt_off;
 };
@@ -60,17 +66,18 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   const int rows = 16 * haf_strips(smax);
   const int h = (smax / 2 + 1) / 2;
   L.c_off = 0;
-  L.p_off = L.c_off + smax * cs * 2;
+  L.p_off = L.c_off + rows * cs * 2;
   L.y_off = L.p_off + rows * ps * 2;
   L.d_off = L.y_off + rows * (h + 1) * 2;
   L.gi_off = L.d_off + 32 * 2;   // 32 ints
   L.acc_off = L.gi_off + 16;
-  L.total = L.acc_off + 4 * (kHafMaxPairs + 1) * 2;
+  L.ring_off = L.acc_off + 4 * (kHafMaxPairs + 1) * 2;
+  L.total = L.ring_off + kHafRing * kHafRingSlot * 2;
   L.total = (L.total + 1) & ~1;  // 16-byte multiple
   L.ca_off = L.m_off = L.ym_off = L.bt_off = 0;
   if (cert) {
     L.ca_off = L.total;
-    L.m_off = L.ca_off + smax * cs * 2;
+    L.m_off = L.ca_off + rows * cs * 2;
     L.ym_off = L.m_off + rows * ps * 2;
     L.bt_off = L.ym_off + rows * (h + 1);
     L.total = L.bt_off + 2 * (kHafMaxPairs + 2);
@@ -85,6 +92,7 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
 template <int NT, int MS>
 __device__ __forceinline__ void power_product(const double* __restrict__ P, const double* __restrict__ Cs, int s,
                                               int cs, int ps, int ntn, int lane, double (&D)[MS][NT][4]) {
+  // P: the previous power (A operand, row stride ps complex); Cs: C (B' source, stride cs)
   constexpr int KS2 = (MS == 1) ? 2 : 1;  // one strip: split K so eight mma chains are in flight
   const int g = lane >> 2, t4 = lane & 3;
   double acc[KS2][MS][NT][4];
@@ -315,8 +323,8 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
   const int ntn = (2 * s + 7) >> 3;  // column tiles in use (<= NT)
   const int hp1 = h + 1;
   double D[MS][NT][4];
-  // power 1 (P = C): p_2 and y_1
-  load_acc<NT, MS>(P, ps, s, lane, D);
+  // power 1 (= C, read in place with stride cs): p_2 and y_1
+  load_acc<NT, MS>(Cs, cs, s, lane, D);
   {
     cplx t = warp_sum_c(even_partial<NT, MS>(D));
     if (lane == 0 && 2 <= n) st_c(acc_p + 4, cadd(ld_c(acc_p + 4), t));
@@ -324,14 +332,17 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
   if (loop) rows_times_d<NT, MS>(D, Dv, Y, 1, hp1, s, lane);
   if constexpr (CERT) {
     double Dm[MS][NT][4];
-    load_acc<NT, MS>(M, ps, s, lane, Dm);
+    load_acc<NT, MS>(Ca, cs, s, lane, Dm);
     double tb = warp_sum_ru(even_bound<NT, MS>(Dm));
     if (lane == 0 && 2 <= n) bT[2] = ru_add(bT[2], tb);
     if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, 1, hp1, s, lane);
   }
   for (int a = 2; a <= h; ++a) {
-    power_product<NT, MS>(P, Cs, s, cs, ps, ntn, lane, D);
-    cplx to = warp_sum_c(odd_partial<NT, MS>(D, P, ps, s, lane));
+    // the previous power: C itself (stride cs) for a = 2, then P (stride ps), in place
+    const double* Q = (a == 2) ? Cs : P;
+    const int qs = (a == 2) ? cs : ps;
+    power_product<NT, MS>(Q, Cs, s, cs, qs, ntn, lane, D);
+    cplx to = warp_sum_c(odd_partial<NT, MS>(D, Q, qs, s, lane));
     cplx te = warp_sum_c(even_partial<NT, MS>(D));
     if (lane == 0) {
       if (2 * a - 1 <= n) st_c(acc_p + 2 * (2 * a - 1), cadd(ld_c(acc_p + 2 * (2 * a - 1)), to));
@@ -341,9 +352,10 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
     store_acc<NT, MS>(P, ps, s, lane, D);
     if (loop) rows_times_d<NT, MS>(D, Dv, Y, a, hp1, s, lane);
     if constexpr (CERT) {
+      const double* Qm = (a == 2) ? Ca : M;
       double Dm[MS][NT][4];
-      power_product<NT, MS>(M, Ca, s, cs, ps, ntn, lane, Dm);
-      double bo = warp_sum_ru(odd_bound<NT, MS>(Dm, M, ps, s, lane));
+      power_product<NT, MS>(Qm, Ca, s, cs, qs, ntn, lane, Dm);
+      double bo = warp_sum_ru(odd_bound<NT, MS>(Dm, Qm, qs, s, lane));
       double be = warp_sum_ru(even_bound<NT, MS>(Dm));
       if (lane == 0) {
         if (2 * a - 1 <= n) bT[2 * a - 1] = ru_add(bT[2 * a - 1], bo);
@@ -361,11 +373,17 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
 // Evaluate the signed power-trace term of one subset `mask` of instance A (N x N
 // complex, row-major, N = 2n even).  Returns the same ball in every lane (radius 0
 // unless CERT).  `loop` selects the loop hafnian; `ws` is this warp's workspace.
+// With `slot` (binary64 tiers): park kg[1..n] and the sign in the ring slot instead
+// of running the Newton recurrence (haf_ring_flush runs it for a whole ring).
 template <bool CERT>
 static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, int n, uint32_t mask,
-                                           bool loop, double* ws, const HafLayout& Lw, int lane) {
+                                           bool loop, double* ws, const HafLayout& Lw, int lane,
+                                           double* slot = nullptr) {
   const int m = __popc(mask);
-  if (m == 0) return cball{mkc(n == 0 ? 1.0 : 0.0, 0.0), 0.0};
+  if (m == 0) {
+    if (slot && lane == 0) st_c(slot, mkc(0.0, 0.0));  // empty subset: term 0 (n >= 1)
+    return cball{mkc(n == 0 ? 1.0 : 0.0, 0.0), 0.0};
+  }
   const int s = 2 * m;
   const int cs = haf_c_stride(s), ps = haf_p_stride(s);
   const int h = (n + 1) / 2, hp1 = h + 1;
@@ -393,22 +411,16 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   }
   __syncwarp();
   const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
-  for (int e = lane; e < s * ccols; e += 32) {
+  // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
+  for (int e = lane; e < rows * ccols; e += 32) {
     const int r = e / ccols, c = e - r * ccols;
     cplx v = mkc(0.0, 0.0);
-    if (c < s) {
+    if (c < s && r < s) {
       const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
       if (loop || rr != cc) v = ld_c(A + ((size_t)rr * N + cc) * 2);
     }
     st_c(Cs + (r * cs + c) * 2, v);
     if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
-  }
-  __syncwarp();
-  for (int e = lane; e < rows * ps; e += 32) {
-    const int r = e / ps, c = e - r * ps;
-    const bool in = r < s && c < s;
-    st_c(P + e * 2, in ? ld_c(Cs + (r * cs + c) * 2) : mkc(0.0, 0.0));
-    if constexpr (CERT) st_c(M + e * 2, in ? ld_c(Ca + (r * cs + c) * 2) : mkc(0.0, 0.0));
   }
   if (loop && lane < s) st_c(Dv + lane * 2, ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2));
   for (int k = lane; k <= n; k += 32) {
@@ -513,6 +525,13 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       }
       st_c(ev + 2 * n, e[n].z);
       eb[0] = e[n].r;
+    } else if (slot) {
+      st_c(slot, mkc(((n - m) & 1) ? -1.0 : 1.0, 0.0));
+      for (int k = 1; k <= n; ++k) {
+        cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
+        if (loop) g = cadd(g, cscale(ld_c(acc_v + 2 * k), (double)k));
+        st_c(slot + 2 * k, g);
+      }
     } else {
       for (int k = 1; k <= n; ++k) {
         cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
@@ -528,11 +547,35 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     }
   }
   __syncwarp();
+  if (!CERT && slot) return cball{mkc(0.0, 0.0), 0.0};
   cplx coeff = ld_c(ev + 2 * n);
   double rad = 0.0;
   if constexpr (CERT) rad = eb[0];
   __syncwarp();
   return cball{((n - m) & 1) ? cneg(coeff) : coeff, rad};
+}
+
+// Run the Newton recurrence of `cnt` parked subsets, one lane each, and return
+// the sum of their signed terms (every lane gets it; fixed butterfly order) and,
+// in *absacc, the sum of |term|.
+__device__ __forceinline__ cplx haf_ring_flush(const double* ring, int cnt, int n, int lane, double* absacc) {
+  cplx term = mkc(0.0, 0.0);
+  if (lane < cnt) {
+    const double* sl = ring + lane * kHafRingSlot * 2;
+    const double sign = sl[0];
+    if (sign != 0.0) {
+      cplx e[kHafMaxPairs + 1];
+      e[0] = mkc(1.0, 0.0);
+      for (int j = 1; j <= n; ++j) {
+        cplx acc = mkc(0.0, 0.0);
+        for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(ld_c(sl + 2 * k), e[j - k]));
+        e[j] = mkc(acc.re / j, acc.im / j);
+      }
+      term = cscale(e[n], sign);
+    }
+  }
+  if (absacc) *absacc = warp_sum_d(cabs_fast(term));
+  return warp_sum_c(term);
 }
 
 }  // namespace gbsb

@@ -168,8 +168,8 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
   } else if (fn == kFnHaf || fn == kFnLhaf) {
     const int n = dim_eval / 2;
     const unsigned long long masks = 1ull << n;
-    // masks per item: 2^9 (binary64) / 2^6 (double-double); smaller instances are one item
-    const int per = tier == kTierDD ? std::min(n, 6) : std::min(n, 9);
+    // masks per item: 2^7 (binary64 tiers) / 2^6 (double-double); smaller instances are one item
+    const int per = tier == kTierDD ? std::min(n, 6) : std::min(n, 7);
     const unsigned long long cnt = 1ull << per;
     for (unsigned long long lo = 0; lo < masks; lo += cnt) add(lo, std::min(cnt, masks - lo));
     P.haf_smax = std::max(P.haf_smax, dim_eval);
@@ -1001,7 +1001,7 @@ namespace gbsb {
 static size_t req_bytes(const SrvReq& r) {
   const size_t d = (size_t)r.dim + 1;
   size_t items = 1;
-  if (r.fn == kFnHaf || r.fn == kFnLhaf) items = (size_t)1 << std::max(0, (int)(d / 2) - 9);
+  if (r.fn == kFnHaf || r.fn == kFnLhaf) items = (size_t)1 << std::max(0, (int)(d / 2) - 7);
   return d * d * 16 + items * 48 + 256;
 }
 
