@@ -125,6 +125,20 @@ int gbs_server_poll(gbs_server* sv, long long ticket, int* done, double* out, do
 int gbs_server_drain(gbs_server* sv, double timeout_s);
 int gbs_server_stats(gbs_server* sv, long long* completed, long long* batches, long long* pending);
 
+/* ---- hafnian without allocation ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory
+ * while they evaluate (their memory belongs to another allocator, or an allocation
+ * would stall a latency-critical loop): d_mats (batch x N x N complex) and d_out
+ * (batch complex) are device pointers the caller owns; every scratch buffer lives
+ * in a fixed 4 MiB __device__ array in the library (held by each GPU that loads it
+ * until exit).  Limits: N <= 32, batch <= 16384, at most 49152 work items
+ * (batch x 2^max(0, N/2 - 7)); larger requests return cudaErrorInvalidValue.  The
+ * first call on a device looks up the array's address (call it before any stream
+ * capture); calls that overlap on the GPU share the array and race.  Asynchronous
+ * on `stream` (a cudaStream_t).  Values equal gbs_haf_host's bit for bit.        */
+int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void* stream);
+const char* gbs_haf_noalloc_last_error(void);
+
 /* ---- measurement ------------------------------------------------------------
  * FP64 tensor-core throughput of this GPU (mma .m16n8k8 .f64 chains on every SM),
  * the denominator of the kernels' roofline fraction.  No reference counterpart.  */
