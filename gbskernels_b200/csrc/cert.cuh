@@ -6,9 +6,10 @@
 // radius r with |x^ - x*| <= r, x* the exact-arithmetic value from the exact binary64
 // input ("ball arithmetic": the midpoint is the ordinary binary64 computation, the
 // radius an upward-rounded running bound).  Reference counterparts:
-// core/certified.cu (perm/haf/lhaf recipes), core/tor_recursive.cu:293-431
-// (recursive-Cholesky torontonian), core/certified_rounding.cuh (the directed
-// rounding helpers; here CUDA's __dadd_ru / __dmul_ru / __ddiv_ru ... are called).
+// core/certified.cu (perm/haf/lhaf recipes), core/certified_rounding.cuh (the
+// directed rounding helpers; here CUDA's __dadd_ru / __dmul_ru / __ddiv_ru ... are
+// called).  The certified torontonian (reference core/tor_recursive.cu:293-431) uses
+// an a-posteriori bound instead and lives in tor_warp.cuh.
 #pragma once
 
 #include "gbs_common.cuh"
@@ -18,10 +19,6 @@ namespace gbsb {
 // u/(1-u) rounded up: bounds u|x*| by kUc|fl(x)| for a rounded result fl(x) of x*.
 constexpr double kUc = 1.1102230246251568e-16;
 
-// Ball in R: midpoint v, radius r.
-struct rball {
-  double v, r;
-};
 // Ball in C: midpoint z, radius r (bound on the complex modulus of the error).
 struct cball {
   cplx z;
@@ -75,139 +72,6 @@ __device__ __forceinline__ cball warp_sum_cb(cball b) {
     b = cb_add(b, o);
   }
   return b;
-}
-
-// ---------------------------------------------------------------------------------
-// Certified recursive prefix-Cholesky torontonian, one lane's subtree (same walk as
-// tor_lane_subtree in perm_tor.cuh).  L and EL are packed lower-triangular (row r at
-// r(r+1)/2); EL[r][c] bounds |L^[r][c] - L*[r][c]|.
-//
-// Entry (r, c), c <= r, with m = (I - O_S)[r][c] (rounded only on the diagonal):
-//   s^ = m - sum_{t<c} L^[r][t] L^[c][t]     (FMA chain, c+1 rounded operations)
-//   e_s = e_m + sum_t (EL_rt |L^_ct| + |L^_rt| EL_ct + EL_rt EL_ct)
-//         + gamma_{c+1} (|m| + sum_t |L^_rt||L^_ct|) + (c+1) ufl
-//   c < r:  L = s^/p^, p^ = L^[c][c] with bound ep < p^:
-//           EL = (e_s + |L| ep) / (p^ - ep) + u|L| + ufl
-//   c = r:  L = sqrt(s^), certifiable iff s^ - e_s > 0:
-//           EL = e_s / sqrt(s^) + u L + ufl   (|sqrt a - sqrt b| = |a-b|/(sqrt a + sqrt b))
-//   det factor (l_xx l_pp)^2 and the running det product are real balls; a leaf
-//   term 1/sqrt(det) is enclosed by [1/sqrt(D^+e), 1/sqrt(D^-e)] with the bounds
-//   computed in outward rounding.  Anything uncertifiable returns false.
-__device__ __forceinline__ double gamma_k(int k) { return gamma_ru((double)k, kU); }
-
-__device__ __forceinline__ bool tor_append_cert(const double* __restrict__ O, int n, int j, int count,
-                                                const int* modes, double* L, double* EL, rball& detf) {
-  const int dim = 2 * n;
-  const int size = 2 * count;
-  for (int t = 0; t < 2; ++t) {
-    const int r = size + t;
-    const int gj = t == 0 ? j : j + n;
-    double* Lr = L + r * (r + 1) / 2;
-    double* ELr = EL + r * (r + 1) / 2;
-    for (int c = 0; c <= r; ++c) {
-      const int mc = ((c >> 1) == count) ? j : modes[c >> 1];
-      const int gc = (c & 1) ? mc + n : mc;
-      const double m = ((gj == gc) ? 1.0 : 0.0) - O[gj * dim + gc];
-      const double em = (gj == gc) ? ru_add(ru_mul(kU, fabs(m)), kUfl) : 0.0;
-      const double* Lc = L + c * (c + 1) / 2;
-      const double* ELc = EL + c * (c + 1) / 2;
-      double s = m;
-      double prop = 0.0, mag = fabs(m);
-      for (int u = 0; u < c; ++u) {
-        const double lr = Lr[u], lc = Lc[u], er = ELr[u], ec = ELc[u];
-        s = fma(-lr, lc, s);
-        prop = ru_add(prop, ru_add(ru_mul(er, fabs(lc)), ru_add(ru_mul(fabs(lr), ec), ru_mul(er, ec))));
-        mag = ru_fma(fabs(lr), fabs(lc), mag);
-      }
-      double es = ru_add(ru_add(em, prop), ru_add(ru_mul(gamma_k(c + 1), mag), ru_mul((double)(c + 1), kUfl)));
-      if (c < r) {
-        const double p = Lc[c], ep = ELc[c];
-        if (!(ep < p)) return false;
-        const double v = s / p;
-        Lr[c] = v;
-        const double den = rd_sub(p, ep);
-        const double av = ru_mul(fabs(v), 1.0 + 4.0 * kU);  // >= |s^/p^|
-        ELr[c] = ru_add(ru_div(ru_add(es, ru_mul(av, ep)), den), ru_add(ru_mul(kU, av), kUfl));
-      } else {
-        if (!(s > 0.0) || !(rd_sub(s, es) > 0.0)) return false;
-        const double v = sqrt(s);
-        Lr[r] = v;
-        ELr[r] = ru_add(ru_div(es, rd_sqrt(s)), ru_add(ru_mul(kUc, v), kUfl));
-      }
-    }
-  }
-  const double a = L[size * (size + 1) / 2 + size], ea = EL[size * (size + 1) / 2 + size];
-  const double b = L[(size + 1) * (size + 2) / 2 + size + 1], eb = EL[(size + 1) * (size + 2) / 2 + size + 1];
-  // ab = a*b, d = ab*ab, real ball products
-  const double ab = a * b;
-  double eab = ru_add(ru_add(ru_mul(fabs(a), eb), ru_mul(fabs(b), ea)), ru_mul(ea, eb));
-  eab = ru_add(eab, ru_add(ru_mul(kUc, fabs(ab)), kUfl));
-  const double d = ab * ab;
-  double ed = ru_add(ru_mul(2.0, ru_mul(fabs(ab), eab)), ru_mul(eab, eab));
-  ed = ru_add(ed, ru_add(ru_mul(kUc, d), kUfl));
-  detf = rball{d, ed};
-  return true;
-}
-
-__device__ __forceinline__ rball rb_mul(rball x, rball y) {
-  rball o;
-  o.v = x.v * y.v;
-  double r = ru_add(ru_add(ru_mul(fabs(x.v), y.r), ru_mul(fabs(y.v), x.r)), ru_mul(x.r, y.r));
-  o.r = ru_add(r, ru_add(ru_mul(kUc, fabs(o.v)), kUfl));
-  return o;
-}
-
-// Leaf term 1 / sqrt(D), D in [D^ - e, D^ + e], D^ > e.  Returns the computed
-// binary64 value and a bound on its distance to 1/sqrt(D*).
-__device__ __forceinline__ bool leaf_cert(rball D, rball& term) {
-  if (!(D.v > 0.0) || !(rd_sub(D.v, D.r) > 0.0)) return false;
-  const double c = 1.0 / sqrt(D.v);
-  const double hi = ru_div(1.0, rd_sqrt(rd_sub(D.v, D.r)));
-  const double lo = __ddiv_rd(1.0, ru_sqrt(ru_add(D.v, D.r)));
-  if (!isfinite(hi) || !isfinite(c)) return false;
-  term = rball{c, fmax(ru_add(hi, -c), rd_sub(c, lo) >= 0.0 ? ru_add(c, -lo) : 0.0)};
-  return true;
-}
-
-static __device__ bool tor_lane_subtree_cert(const double* __restrict__ O, int n, int g, uint32_t pat, double* L,
-                                      double* EL, double& total, double& bound) {
-  int modes[32];
-  rball detat[33];
-  int count = 0;
-  detat[0] = rball{1.0, 0.0};
-  for (int j = 0; j < g; ++j) {
-    if (!((pat >> j) & 1u)) continue;
-    modes[count] = j;
-    rball df;
-    if (!tor_append_cert(O, n, j, count, modes, L, EL, df)) return false;
-    detat[count + 1] = rb_mul(detat[count], df);
-    ++count;
-  }
-  const int pc = count, r = n - g;
-  double tot = 0.0, bnd = 0.0;
-  {
-    rball t;
-    if (!leaf_cert(detat[pc], t)) return false;
-    tot = ((n - pc) & 1) ? -t.v : t.v;
-    bnd = t.r;
-  }
-  const uint64_t nT = 1ull << r;
-  for (uint64_t Tm = 1; Tm < nT; ++Tm) {
-    const int z = __ffsll((long long)Tm) - 1;
-    const int jz = g + r - 1 - z;
-    const int cnt0 = pc + __popcll((long long)(Tm >> (z + 1)));
-    modes[cnt0] = jz;
-    rball df;
-    if (!tor_append_cert(O, n, jz, cnt0, modes, L, EL, df)) return false;
-    detat[cnt0 + 1] = rb_mul(detat[cnt0], df);
-    rball t;
-    if (!leaf_cert(detat[cnt0 + 1], t)) return false;
-    tot = ((n - cnt0 - 1) & 1) ? tot - t.v : tot + t.v;
-    bnd = ru_add(ru_add(bnd, t.r), ru_add(ru_mul(kUc, fabs(tot)), kUfl));
-  }
-  total = tot;
-  bound = bnd;
-  return true;
 }
 
 // ---------------------------------------------------------------------------------

@@ -15,6 +15,7 @@
 #include "haf_pt.cuh"
 #include "perm_tor.cuh"
 #include "cert.cuh"
+#include "tor_warp.cuh"
 
 namespace gbsb {
 
@@ -100,11 +101,27 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     }
     r.val = acc;
   } else if (TIER == kTierCert) {
+    // same grouping as the binary64 tiers (rings of kHafRing subsets, butterfly sum
+    // per ring) so the certified value is the fp64 value bit for bit
     const HafLayout L = haf_layout(haf_smax, true);
+    double* ring = ws + L.ring_off;
     cball acc{mkc(0.0, 0.0), 0.0};
+    int cnt = 0;
     for (unsigned long long k = 0; k < w.count; ++k) {
       cball t = haf_subset_term_tc<true>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
-      acc = cb_add(acc, t);
+      if (lane == 0) {
+        ring[cnt * 3] = t.z.re;
+        ring[cnt * 3 + 1] = t.z.im;
+        ring[cnt * 3 + 2] = t.r;
+      }
+      if (++cnt == kHafRing || k + 1 == w.count) {
+        __syncwarp();
+        cball b{mkc(0.0, 0.0), 0.0};
+        if (lane < cnt) b = cball{mkc(ring[lane * 3], ring[lane * 3 + 1]), ring[lane * 3 + 2]};
+        acc = cb_add(acc, warp_sum_cb(b));
+        cnt = 0;
+        __syncwarp();
+      }
     }
     r.val = ddc_from_c(acc.z);
     r.aux = acc.r;
@@ -141,46 +158,61 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
   ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStOk};
   const int n = d.dim / 2;
   const int dim = d.dim;
-  // stage the real part of O in this warp's shared workspace (row-major doubles)
   const double* Oc = mats + d.off;
+  if (TIER != kTierDD) {
+    // binary64 tiers: warp-cooperative prefix walk with the 32-subset register tail
+    // (tor_warp.cuh); one work item = w.count prefix patterns over the first d.param
+    // prefix modes, walked one after another by the whole warp
+    const TorWLayout Lw = tor_w_layout(n, TIER == kTierCert);
+    double* rho = ws + Lw.rho_off;
+    bool proved = true;
+    if (TIER == kTierCert) {
+      double dmin2 = 0.0;
+      const double sigma = tor_cert_sigma(Oc, n, ws + Lw.col_off, lane, dmin2);
+      proved = sigma > 0.0;
+      tor_cert_rho(sigma, dmin2, n, rho, lane);
+    }
+    double val = 0.0, aux = 0.0;
+    bool ok = true;
+    if (proved) {
+      for (unsigned long long p = 0; p < w.count; ++p) {
+        double t = 0.0, a = 0.0;
+        ok = tor_warp_item<TIER == kTierKappa, TIER == kTierCert>(Oc, n, d.param, (uint32_t)(w.lo + p), ws, Lw,
+                                                                   rho, lane, t, a) && ok;
+        if (p == 0) {
+          val = t;
+          aux = a;
+        } else if (TIER == kTierCert) {
+          val += t;
+          aux = ru_add(ru_add(aux, a), ru_mul(kUc, fabs(val)));
+        } else {
+          val += t;
+          aux += a;
+        }
+      }
+    }
+    r.val = ddc{dd_make(val), dd_make(0.0)};
+    r.aux = aux;
+    if (!proved || !ok) r.st = TIER == kTierCert ? kStUncertified : kStOffDomain;
+    __syncwarp();
+    return r;
+  }
+  // double-double tier: one lane per prefix pattern, each walking its own subtree
+  // (perm_tor.cuh); the real part of O is staged in the warp's shared workspace
   for (int e = lane; e < dim * dim; e += 32) ws[e] = Oc[2 * e];
   __syncwarp();
   const bool active = (unsigned long long)lane < w.count;
   const uint32_t pat = (uint32_t)(w.lo + lane);
   bool ok = true;
   double absacc = 0.0;
-  if (TIER == kTierCert) {
-    double total = 0.0, bnd = 0.0;
-    if (active) {
-      double L[kTorPackedMax], EL[kTorPackedMax];
-      ok = tor_lane_subtree_cert(ws, n, d.param, pat, L, EL, total, bnd);
-    }
-    cball b{mkc(ok ? total : 0.0, 0.0), ok ? bnd : 0.0};
-    b = warp_sum_cb(b);
-    r.val = ddc{dd_make(b.z.re), dd_make(0.0)};
-    r.aux = b.r;
-  } else if (TIER == kTierDD) {
-    dd total = dd_make(0.0);
-    if (active) {
-      dd L[kTorPackedMax];
-      ok = tor_lane_subtree<dd>(ws, n, d.param, pat, L, total, absacc, false);
-    }
-    dd v = ok ? total : dd_make(0.0);
-    ddc c = ddc{v, dd_make(0.0)};
-    c = warp_sum_ddc(c);
-    r.val = c;
-  } else {
-    double total = 0.0;
-    if (active) {
-      double L[kTorPackedMax];
-      ok = tor_lane_subtree<double>(ws, n, d.param, pat, L, total, absacc, TIER == kTierKappa);
-    }
-    double v = warp_sum_d(ok ? total : 0.0);
-    r.val = ddc{dd_make(v), dd_make(0.0)};
-    r.aux = warp_sum_d(absacc);
+  dd total = dd_make(0.0);
+  if (active) {
+    dd L[kTorPackedMax];
+    ok = tor_lane_subtree<dd>(ws, n, d.param, pat, L, total, absacc, false);
   }
-  const bool all_ok = __all_sync(0xffffffffu, ok);
-  if (!all_ok) r.st = TIER == kTierCert ? kStUncertified : kStOffDomain;
+  const dd v = ok ? total : dd_make(0.0);
+  r.val = warp_sum_ddc(ddc{v, dd_make(0.0)});
+  if (!__all_sync(0xffffffffu, ok)) r.st = kStOffDomain;
   __syncwarp();
   return r;
 }

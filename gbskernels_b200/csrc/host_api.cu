@@ -28,6 +28,7 @@
 #include "gbs_kernels.cuh"
 #include "haf_dd.cuh"
 #include "haf_pt.cuh"
+#include "tor_warp.cuh"
 
 namespace gbsb {
 
@@ -126,11 +127,18 @@ struct Plan {
 
 
 // Cost model (relative units) used only to order the queue heaviest-first.
-static double item_cost(int fn, int dim, unsigned long long count, int tier) {
+static double item_cost(int fn, int dim, unsigned long long count, int tier, int param) {
   double c;
   switch (fn) {
     case kFnPerm: c = (double)count * dim; break;
-    case kFnTor: { int n = dim / 2; c = (double)count * std::ldexp(1.0, n) * n * n / 32.0; break; }
+    case kFnTor: {
+      // binary64 tiers: count prefix patterns, 2^(q - g) leaves of 32 subsets each
+      // (g = param); double-double: count lanes of 2^(n - g) subsets each
+      const int n = dim / 2, q = n - std::min(n, 5);
+      c = tier == kTierDD ? (double)count * std::ldexp(1.0, n - param) * n * n
+                          : (double)count * std::ldexp(1.0, q - param) * 32.0 * (36.0 * q + 1400.0);
+      break;
+    }
     default: { double n = dim / 2.0; c = (double)count * (n + 1) * n * n * n; break; }
   }
   return tier == kTierDD ? 20.0 * c : c;
@@ -173,12 +181,19 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     const unsigned long long cnt = 1ull << per;
     for (unsigned long long lo = 0; lo < masks; lo += cnt) add(lo, std::min(cnt, masks - lo));
     P.haf_smax = std::max(P.haf_smax, dim_eval);
-  } else {  // tor
+  } else if (tier == kTierDD) {  // tor, double-double: one lane per prefix pattern
     const int n = dim_eval / 2;
-    const int rcap = tier == kTierDD ? 7 : 10;
-    const int g = std::max(std::min(n, 5), n - rcap);
+    const int g = std::max(std::min(n, 5), n - 7);
     const unsigned long long pats = 1ull << g;
     for (unsigned long long lo = 0; lo < pats; lo += 32) add(lo, std::min<unsigned long long>(32, pats - lo));
+    d.param = g;
+  } else {  // tor, binary64 tiers: one warp per prefix pattern over the first g prefix modes
+    const int n = dim_eval / 2;
+    const int q = n - std::min(n, 5);
+    // 2^9 leaves (x 32 tail subsets) per item; 2^10 for the certified tier, whose
+    // items also repeat the per-instance eigenvalue proof
+    const int g = std::max(0, q - (tier == kTierCert ? 10 : 9));
+    for (unsigned long long p = 0; p < (1ull << g); ++p) add(p, 1);
     d.param = g;
   }
   d.nitems = (int)P.items.size() - d.item0;
@@ -193,7 +208,7 @@ static int ws_for_plan(const Plan& P) {
     const int fn = d.ft >> 2, tier = d.ft & 3;
     int w = 0;
     if (fn == kFnPerm) w = 2 * d.dim * d.dim;
-    else if (fn == kFnTor) w = d.dim * d.dim;
+    else if (fn == kFnTor) w = tier == kTierDD ? d.dim * d.dim : tor_w_layout(d.dim / 2, tier == kTierCert).total;
     else if (tier == kTierDD) w = haf_dd_layout(P.haf_smax).total;
     else w = haf_layout(P.haf_smax, tier == kTierCert).total;
     ws = std::max(ws, w);
@@ -407,7 +422,7 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
       std::vector<double> c(ni);
       for (int k = 0; k < ni; ++k) {
         const InstDesc& d = P.insts[k];
-        c[k] = item_cost(d.ft >> 2, d.dim, P.items[d.item0].count, d.ft & 3);
+        c[k] = item_cost(d.ft >> 2, d.dim, P.items[d.item0].count, d.ft & 3, d.param);
       }
       std::stable_sort(inst_order.begin(), inst_order.end(), [&](int a, int b) { return c[a] > c[b]; });
     }

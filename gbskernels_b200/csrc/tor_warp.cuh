@@ -1,0 +1,501 @@
+// tor_warp.cuh -- torontonian by a warp-cooperative prefix-Cholesky walk with a
+// 32-subset register tail per prefix leaf (binary64, kappa and certified tiers).
+//
+// tor(O) = sum_{S subset [k]} (-1)^(k-|S|) / sqrt(det((I - O)_S)),  xxpp ordering,
+// where including mode j puts rows / columns j and j + k of M = I - O in the minor.
+// Reference algorithm: the recursive prefix Cholesky of core/tor_recursive.cu:41-115
+// (cpu_ref/tor_recursive.py:46-100): the subsets are walked in binary-counter order,
+// including a mode appends its two rows to one Cholesky factor, det = prod of the
+// squared pivots.
+//
+// B200 mapping (this repository's design):
+//   * the last r = min(k, 5) modes form the TAIL, the first q = k - r the PREFIX.
+//     The tail rows sit at the bottom of every column of the factor: for a prefix
+//     subset S with factor L of M_S, column u holds L[t][u] (prefix rows t > u)
+//     followed by W[u][.] = (L^{-1} M_{S,T})[u][.], and the Schur complement
+//     Z = M_TT - W^T W is kept per depth (Zd[c] after c prefix modes), updated by
+//     the two new W rows of each append;
+//   * one warp walks the prefix subsets of a work item (a fixed pattern over the
+//     first g prefix modes, then all subsets of the prefix modes [g, q)).  Appending
+//     a mode computes its two factor rows and two W rows in one forward substitution:
+//     lanes own residual slots x (prefix columns, the two new diagonal slots, the
+//     2r tail columns), the owner of step v scales its residual by 1 / L[v][v] and
+//     broadcasts it, every lane updates with column v (contiguous in shared memory);
+//   * at every prefix leaf, lane l takes the tail subset T' = l: Z~ = Z with the
+//     rows / columns of the excluded tail modes replaced by the identity (the same
+//     determinant, and the same rounded operations as factoring the compressed
+//     matrix, since the extra terms are exact zeros), factored in registers, and the
+//     32 signed terms are summed by a fixed butterfly;
+//   * the factor, Zd and the pivot reciprocals live in the warp's shared workspace
+//     (about 18 KB at 24 modes): no local memory.
+//
+// Certified tier: the binary64 walk is the fp64 tier's (bit-identical value) and each
+// term gets an a-posteriori radius.  For a subset of dimension m the computed factor
+// satisfies L^L^T = A + F with |F_ij| <= c_m D_i D_j (Cholesky backward error,
+// gamma_{m+2}, reciprocal-multiply counted; D_i = fl(sqrt(fl(1 - O_ii)))), so
+// det(L^)^2 = det(A) det(I + X) with ||X|| <= eta_m = m c_m / sigma, sigma a rigorous
+// lower bound of lambda_min(D^-1 M D^-1) -- valid for every principal submatrix by
+// Cauchy interlacing, so ONE bound per instance certifies all 2^k subsets.  sigma is
+// proved per instance by a binary64 Cholesky of D^-1 M D^-1 - sigma I that succeeds
+// (success implies lambda_min >= -gamma_{m+2} tr / (1 - gamma_{m+2}), Weyl for the
+// rounding of the scaled matrix).  The term radius is |t^| rho_m with rho_m from the
+// eta_m, pivot-product and final sqrt / division roundings (tor_cert_rho).
+#pragma once
+
+#include "cert.cuh"
+#include "gbs_common.cuh"
+
+namespace gbsb {
+
+constexpr int kTorTail = 5;                        // tail modes (2^5 subsets = 32 lanes)
+constexpr int kTorTD = 2 * kTorTail;               // tail rows (10)
+constexpr int kTorZE = kTorTD * (kTorTD + 1) / 2;  // packed lower tail entries (55)
+
+struct TorWLayout {
+  int col_off, inv_off, zd_off, det_off, gidx_off, rho_off, total;  // in doubles
+};
+
+// rows = 2q prefix rows; column u holds rows - u prefix slots + 10 tail slots.
+__host__ __device__ inline int tor_col_base(int u, int rows) { return u * (rows + kTorTD) - (u * (u - 1)) / 2; }
+
+__host__ __device__ inline TorWLayout tor_w_layout(int kmax, bool cert) {
+  TorWLayout Lw;
+  const int q = kmax > kTorTail ? kmax - kTorTail : 0;
+  const int rows = 2 * q;
+  Lw.col_off = 0;
+  Lw.inv_off = Lw.col_off + tor_col_base(rows, rows) + 1;
+  Lw.zd_off = Lw.inv_off + rows + 1;
+  Lw.det_off = Lw.zd_off + (q + 1) * kTorZE;
+  Lw.gidx_off = Lw.det_off + q + 2;
+  Lw.rho_off = Lw.gidx_off + (rows + 2) / 2;
+  int total = Lw.rho_off + (cert ? 2 * kmax + 2 : 0);
+  if (cert) {  // the sigma proof factors a packed 2k x 2k matrix in the col / zd region
+    const int need = (2 * kmax) * (2 * kmax + 1) / 2 + 8;
+    if (Lw.det_off < need) {
+      const int shift = need - Lw.det_off;
+      Lw.det_off += shift;
+      Lw.gidx_off += shift;
+      Lw.rho_off += shift;
+      total += shift;
+    }
+  }
+  Lw.total = (total + 3) & ~3;
+  return Lw;
+}
+
+__device__ __forceinline__ double tor_m(const double* __restrict__ Oc, int dim, int a, int b) {
+  // entry of M = I - O from the complex-interleaved input (real part)
+  const double o = Oc[2 * (a * dim + b)];
+  return a == b ? 1.0 - o : -o;
+}
+
+// global component index of tail row jt (x of mode q + jt/2, or its p)
+__device__ __forceinline__ int tor_tail_g(int jt, int q, int k) { return (jt & 1) ? q + (jt >> 1) + k : q + (jt >> 1); }
+
+// packed lower index e -> (row i, column jj), i >= jj, i < 10
+__device__ __forceinline__ void tor_tri_ij(int e, int& i, int& jj) {
+  i = 0;
+  while ((i + 1) * (i + 2) / 2 <= e) ++i;
+  jj = e - i * (i + 1) / 2;
+}
+
+// Append prefix mode j (global components j and j + k) as rows R0 = 2c, R1 = 2c + 1.
+// Writes the two factor rows into columns 0..R0 (and L[R1][R0]), the two W rows
+// into the tail slots of columns R0 and R1, inv[R0], inv[R1], detat[c + 1] and
+// Zd[c + 1].  Returns false when a pivot is not positive (the walk continues with a
+// unit pivot; the instance is flagged).
+__device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int k, int q, int r, int j, int c,
+                                             double* col, double* inv, double* zd, double* detat, int* gidx,
+                                             int lane) {
+  const int dim = 2 * k;
+  const int rows = 2 * q;
+  const int R0 = 2 * c, R1 = R0 + 1;
+  const int gR0 = j, gR1 = j + k;
+  const int nx = R0 + 2 + 2 * r;
+  if (lane == 0) {
+    gidx[R0] = gR0;
+    gidx[R1] = gR1;
+  }
+  // residual slots x = lane, lane + 32
+  double a[2], b[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int x = lane + 32 * h;
+    a[h] = 0.0;
+    b[h] = 0.0;
+    if (x < R0) {
+      const int gc = gidx[x];
+      a[h] = tor_m(Oc, dim, gR0, gc);
+      b[h] = tor_m(Oc, dim, gR1, gc);
+    } else if (x == R0) {
+      a[h] = tor_m(Oc, dim, gR0, gR0);
+      b[h] = tor_m(Oc, dim, gR1, gR0);
+    } else if (x == R1) {
+      b[h] = tor_m(Oc, dim, gR1, gR1);
+    } else if (x < nx) {
+      const int gT = tor_tail_g(x - R0 - 2, q, k);
+      a[h] = tor_m(Oc, dim, gR0, gT);
+      b[h] = tor_m(Oc, dim, gR1, gT);
+    }
+  }
+  // forward substitution over the existing columns v < R0
+  for (int v = 0; v < R0; ++v) {
+    const int owner = v & 31;
+    double* cv = col + tor_col_base(v, rows);
+    double l0 = 0.0, l1 = 0.0;
+    if (lane == owner) {
+      const double iv = inv[v];
+      l0 = ((v >> 5) ? a[1] : a[0]) * iv;
+      l1 = ((v >> 5) ? b[1] : b[0]) * iv;
+      cv[R0 - v] = l0;
+      cv[R1 - v] = l1;
+    }
+    l0 = __shfl_sync(0xffffffffu, l0, owner);
+    l1 = __shfl_sync(0xffffffffu, l1, owner);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int x = lane + 32 * h;
+      double e;
+      bool upd = true;
+      if (x < R0) {
+        upd = x > v;
+        e = upd ? cv[x - v] : 0.0;
+      } else if (x == R0) {
+        e = l0;
+      } else if (x == R1) {
+        e = l1;
+      } else if (x < nx) {
+        e = cv[rows - v + (x - R0 - 2)];
+      } else {
+        upd = false;
+        e = 0.0;
+      }
+      if (upd) {
+        a[h] = fma(-e, l0, a[h]);
+        b[h] = fma(-e, l1, b[h]);
+      }
+    }
+  }
+  // the two diagonal slots
+  const int o0 = R0 & 31, h0 = R0 >> 5;
+  const int o1 = R1 & 31, h1 = R1 >> 5;
+  double s0 = __shfl_sync(0xffffffffu, h0 ? a[1] : a[0], o0);
+  const double m10 = __shfl_sync(0xffffffffu, h0 ? b[1] : b[0], o0);
+  bool ok = s0 > 0.0;
+  if (!ok) s0 = 1.0;
+  const double i0 = 1.0 / sqrt(s0);
+  const double l10 = m10 * i0;
+  double s1 = fma(-l10, l10, __shfl_sync(0xffffffffu, h1 ? b[1] : b[0], o1));
+  if (!(s1 > 0.0)) {
+    ok = false;
+    s1 = 1.0;
+  }
+  const double i1 = 1.0 / sqrt(s1);
+  double* c0 = col + tor_col_base(R0, rows);
+  double* c1 = col + tor_col_base(R1, rows);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int x = lane + 32 * h;
+    if (x >= R0 + 2 && x < nx) {
+      const int jt = x - R0 - 2;
+      const double w0 = a[h] * i0;
+      const double w1 = fma(-w0, l10, b[h]) * i1;
+      c0[rows - R0 + jt] = w0;
+      c1[rows - R1 + jt] = w1;
+    }
+  }
+  if (lane == 0) {
+    c0[1] = l10;
+    inv[R0] = i0;
+    inv[R1] = i1;
+    detat[c + 1] = detat[c] * s0 * s1;
+  }
+  __syncwarp();
+  // Zd[c + 1] = Zd[c] - w0 w0^T - w1 w1^T  (packed lower, tail rows < 2r)
+  const double* zs = zd + c * kTorZE;
+  double* zt = zd + (c + 1) * kTorZE;
+  const double* w0p = c0 + rows - R0;
+  const double* w1p = c1 + rows - R1;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int e = lane + 32 * h;
+    if (e < kTorZE) {
+      int i, jj;
+      tor_tri_ij(e, i, jj);
+      double z = zs[e];
+      if (i < 2 * r) {
+        z = fma(-w0p[i], w0p[jj], z);
+        z = fma(-w1p[i], w1p[jj], z);
+      }
+      zt[e] = z;
+    }
+  }
+  __syncwarp();
+  return ok;
+}
+
+// One prefix leaf: every lane l < 2^r factors Z~ for the tail subset l.  Returns the
+// lane's signed term (0 for idle lanes); ok is cleared on a non-positive pivot and
+// the term dimension m = 2 (c + |T'|) is returned for the certified radius.
+__device__ __forceinline__ double tor_w_leaf(const double* zc, int r, int c, int k, double detc, int lane,
+                                             bool& ok, int& m) {
+  double term = 0.0;
+  m = 0;
+  if (lane < (1 << r)) {
+    const int td = 2 * r;
+    double Lz[kTorZE];
+    double iv[kTorTD];
+    double det = 1.0;
+#pragma unroll
+    for (int i = 0; i < kTorTD; ++i) {
+      const bool in_i = i < td && ((lane >> (i >> 1)) & 1);
+#pragma unroll
+      for (int jj = 0; jj <= i; ++jj) {
+        const bool in_j = jj < td && ((lane >> (jj >> 1)) & 1);
+        const int e = i * (i + 1) / 2 + jj;
+        double s = (in_i && in_j) ? zc[e] : (i == jj ? 1.0 : 0.0);
+#pragma unroll
+        for (int u = 0; u < jj; ++u) s = fma(-Lz[i * (i + 1) / 2 + u], Lz[jj * (jj + 1) / 2 + u], s);
+        if (jj < i) {
+          Lz[e] = s * iv[jj];
+        } else {
+          if (!(s > 0.0)) {
+            ok = false;
+            s = 1.0;
+          }
+          const double d = sqrt(s);
+          Lz[e] = d;
+          iv[i] = 1.0 / d;
+          det *= s;
+        }
+      }
+    }
+    const int nin = __popc(lane);
+    m = 2 * (c + nin);
+    const double t = 1.0 / sqrt(detc * det);
+    term = ((k - c - nin) & 1) ? -t : t;
+  }
+  return term;
+}
+
+// ------------------------------------------------------------ certified prologue
+// Rigorous lower bound sigma of lambda_min(D^-1 M D^-1), D_i = fl(sqrt(fl(1 - O_ii))),
+// for the whole 2k x 2k matrix; <= 0 when none could be proved.  Also returns a lower
+// bound of min D_i^2 for the underflow term.  Scratch: packed lower (2k)(2k+1)/2
+// doubles at S (warp-private shared memory).
+static __device__ double tor_cert_sigma(const double* __restrict__ Oc, int k, double* S, int lane, double& dmin2) {
+  const int dim = 2 * k;
+  const int np = dim * (dim + 1) / 2;
+  double dm = 1e300;
+  bool okd = true;
+  for (int i = lane; i < dim; i += 32) {
+    const double mii = 1.0 - Oc[2 * (i * dim + i)];
+    if (!(mii > 0.0)) okd = false;
+    const double di = mii > 0.0 ? sqrt(mii) : 0.0;
+    dm = fmin(dm, __dmul_rd(di, di));
+  }
+  okd = __all_sync(0xffffffffu, okd);
+#pragma unroll
+  for (int mm = 16; mm > 0; mm >>= 1) dm = fmin(dm, shfl_xor_d(dm, mm));
+  dmin2 = dm;
+  if (!okd) return -1.0;
+  auto hval = [&](int i, int jj) {
+    const double di = sqrt(1.0 - Oc[2 * (i * dim + i)]);
+    const double dj = sqrt(1.0 - Oc[2 * (jj * dim + jj)]);
+    return tor_m(Oc, dim, i, jj) / di / dj;
+  };
+  auto unpack = [&](int e, int& i, int& jj) {
+    i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while (i * (i + 1) / 2 > e) --i;
+    while ((i + 1) * (i + 2) / 2 <= e) ++i;
+    jj = e - i * (i + 1) / 2;
+  };
+  // ||H^||_F (upward); H^ = fl(fl(m_ij / D_i) / D_j) is within gamma_3 |h| of the
+  // exact scaled entry, so ||E_H||_F <= gamma_3 / (1 - gamma_3) ||H^||_F
+  double fro2 = 0.0;
+  for (int e = lane; e < np; e += 32) {
+    int i, jj;
+    unpack(e, i, jj);
+    const double h = hval(i, jj);
+    fro2 = ru_fma(h, h, fro2);
+    if (i != jj) fro2 = ru_fma(h, h, fro2);
+  }
+  fro2 = warp_sum_ru(fro2);
+  const double g3 = gamma_ru(3.0, kU);
+  const double eh = ru_mul(ru_div(g3, rd_sub(1.0, g3)), ru_sqrt(fro2));
+  const double gm = gamma_ru((double)(dim + 2), kU);
+  // one attempt: factor B = fl(H^ - sig I) in place (right-looking, packed lower);
+  // on success return the proved bound sig - tau - ||E||, else -1
+  auto attempt = [&](double sig) -> double {
+    double trace = 0.0;
+    for (int e = lane; e < np; e += 32) {
+      int i, jj;
+      unpack(e, i, jj);
+      double h = hval(i, jj);
+      if (i == jj) {
+        h = h - sig;
+        trace = ru_add(trace, fabs(h));
+      }
+      S[e] = h;
+    }
+    trace = warp_sum_ru(trace);
+    __syncwarp();
+    for (int jc = 0; jc < dim; ++jc) {
+      const double p = S[jc * (jc + 1) / 2 + jc];
+      if (!(p > 0.0)) {  // warp-uniform (every lane read the same word)
+        __syncwarp();
+        return -1.0;
+      }
+      const double id = 1.0 / sqrt(p);
+      __syncwarp();
+      for (int i = jc + 1 + lane; i < dim; i += 32) S[i * (i + 1) / 2 + jc] *= id;
+      __syncwarp();
+      for (int i = jc + 1; i < dim; ++i) {
+        const double lij = S[i * (i + 1) / 2 + jc];
+        for (int l = jc + 1 + lane; l <= i; l += 32)
+          S[i * (i + 1) / 2 + l] = fma(-lij, S[l * (l + 1) / 2 + jc], S[i * (i + 1) / 2 + l]);
+      }
+      __syncwarp();
+    }
+    // success: lambda_min(B) >= -tau, tau = gm tr(B) / (1 - gm); the distance of B to
+    // the exact H - sig I is at most eh + u sum |b_ii| (rounding of the diagonal shift)
+    const double tau = ru_div(ru_mul(gm, trace), rd_sub(1.0, gm));
+    const double err = ru_add(eh, ru_mul(kUc, trace));
+    return rd_sub(rd_sub(sig, tau), err);
+  };
+  // halve sig from 1/2 until a factorisation succeeds, then three bisection steps
+  double best = -1.0, sig = 0.5, fail_at = 1.0;
+  for (int t = 0; t < 40 && best <= 0.0; ++t) {
+    const double c = attempt(sig);
+    if (c > 0.0) {
+      best = c;
+    } else {
+      fail_at = sig;
+      sig *= 0.5;
+    }
+  }
+  if (best <= 0.0) return -1.0;
+  double lo = sig, hi = fail_at;
+  for (int b = 0; b < 3; ++b) {
+    const double mid = 0.5 * (lo + hi);
+    const double c = attempt(mid);
+    if (c > 0.0) {
+      lo = mid;
+      best = fmax(best, c);
+    } else {
+      hi = mid;
+    }
+  }
+  return best;
+}
+
+// rho_m for m = 0..2k (a-posteriori relative radius of one term of dimension m),
+// written to rho[]; +inf where m * eta_m is not below 1/2.
+//   c_m   = (g/(1-g) + u/(1-u)) / (1-u)^2 + (m+2) ufl / dmin2,  g = gamma_{m+2}
+//   eta_m = m c_m / sigma
+//   t / t^ lies in [Lo, Up] with
+//   Up = sqrt((1 + gamma_{m+1}) / ((1 - m eta)(1 - 2mu))) (1+u)/(1-u)
+//   Lo = sqrt((1 - gamma_{m+1})(1 - m eta)(1 - 2mu)) (1-u)/(1+u)
+// (pivot product: m+1 roundings; fl(sqrt) of each pivot squared: (1 +- u)^{2m};
+// det(I + X) within (1 -+ eta)^m; the final sqrt and division), rho = max(Up-1, 1-Lo).
+static __device__ void tor_cert_rho(double sigma, double dmin2, int k, double* rho, int lane) {
+  for (int m = lane; m <= 2 * k; m += 32) {
+    double out;
+    if (m == 0) {
+      out = 0.0;  // empty minor: t = 1 exactly
+    } else if (!(sigma > 0.0) || !(dmin2 > 0.0)) {
+      out = INFINITY;
+    } else {
+      const double md = (double)m;
+      const double g = gamma_ru(md + 2.0, kU);
+      double cm = ru_add(ru_div(g, rd_sub(1.0, g)), ru_div(kU, rd_sub(1.0, kU)));
+      cm = ru_div(cm, __dmul_rd(rd_sub(1.0, kU), rd_sub(1.0, kU)));
+      cm = ru_add(cm, ru_div(ru_mul(md + 2.0, kUfl), dmin2));
+      const double eta = ru_div(ru_mul(md, cm), sigma);
+      const double meta = ru_mul(md, eta);
+      if (!(meta < 0.5)) {
+        out = INFINITY;
+      } else {
+        const double gp = gamma_ru(md + 1.0, kU);
+        const double two_mu = ru_mul(2.0 * md, kU);
+        const double den = __dmul_rd(rd_sub(1.0, meta), rd_sub(1.0, two_mu));
+        double up = ru_sqrt(ru_div(ru_add(1.0, gp), den));
+        up = ru_div(ru_mul(up, ru_add(1.0, kU)), rd_sub(1.0, kU));
+        double lo = rd_sqrt(__dmul_rd(rd_sub(1.0, gp), den));
+        lo = __ddiv_rd(__dmul_rd(lo, rd_sub(1.0, kU)), ru_add(1.0, kU));
+        out = fmax(ru_add(up, -1.0), ru_add(1.0, -lo));
+      }
+    }
+    rho[m] = out;
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------ one work item
+// Prefix pattern `pat` over the first g prefix modes, then every subset of the
+// prefix modes [g, q) with its 2^r tail subsets.  KAPPA adds sum |term|, CERT the
+// ball radius (aux).  Returns false when a pivot was not positive.
+template <bool KAPPA, bool CERT>
+static __device__ bool tor_warp_item(const double* __restrict__ Oc, int k, int g, uint32_t pat, double* ws,
+                              const TorWLayout& Lw, const double* rho, int lane, double& total, double& aux) {
+  const int dim = 2 * k;
+  const int r = k < kTorTail ? k : kTorTail;
+  const int q = k - r;
+  double* col = ws + Lw.col_off;
+  double* inv = ws + Lw.inv_off;
+  double* zd = ws + Lw.zd_off;
+  double* detat = ws + Lw.det_off;
+  int* gidx = reinterpret_cast<int*>(ws + Lw.gidx_off);
+  // Zd[0] = M_TT (packed lower, tail rows < 2r; the rest unused)
+  for (int e = lane; e < kTorZE; e += 32) {
+    int i, jj;
+    tor_tri_ij(e, i, jj);
+    zd[e] = (i < 2 * r) ? tor_m(Oc, dim, tor_tail_g(i, q, k), tor_tail_g(jj, q, k)) : 0.0;
+  }
+  if (lane == 0) detat[0] = 1.0;
+  __syncwarp();
+  bool ok = true;
+  int count = 0;
+  for (int j = 0; j < g; ++j)
+    if ((pat >> j) & 1u) {
+      ok = tor_w_append(Oc, k, q, r, j, count, col, inv, zd, detat, gidx, lane) && ok;
+      ++count;
+    }
+  const int pc = count;
+  double sum = 0.0, sabs = 0.0, srad = 0.0;
+  const int rp = q - g;
+  const uint64_t nT = 1ull << rp;
+  for (uint64_t Tm = 0; Tm < nT; ++Tm) {
+    if (Tm) {
+      // counter bit b <-> prefix mode g + rp - 1 - b (lowest bit = last prefix mode)
+      const int z = __ffsll((long long)Tm) - 1;
+      const int jz = g + rp - 1 - z;
+      count = pc + __popcll((long long)(Tm >> (z + 1)));
+      ok = tor_w_append(Oc, k, q, r, jz, count, col, inv, zd, detat, gidx, lane) && ok;
+      ++count;
+    }
+    int m = 0;
+    const double t = tor_w_leaf(zd + count * kTorZE, r, count, k, detat[count], lane, ok, m);
+    if (CERT) {
+      // ball butterfly: the value operations are those of warp_sum_d
+      double v = t;
+      double rr = (t != 0.0) ? ru_add(ru_mul(fabs(t), rho[m]), kUfl) : 0.0;
+#pragma unroll
+      for (int mm = 16; mm > 0; mm >>= 1) {
+        const double ov = shfl_xor_d(v, mm), orr = shfl_xor_d(rr, mm);
+        v += ov;
+        rr = ru_add(ru_add(rr, orr), ru_mul(kUc, fabs(v)));
+      }
+      sum += v;
+      srad = ru_add(ru_add(srad, rr), ru_mul(kUc, fabs(sum)));
+    } else {
+      sum += warp_sum_d(t);
+      if (KAPPA) sabs += warp_sum_d(fabs(t));
+    }
+  }
+  total = sum;
+  aux = CERT ? srad : sabs;
+  return __all_sync(0xffffffffu, ok);
+}
+
+}  // namespace gbsb
