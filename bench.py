@@ -324,7 +324,13 @@ def main():
                        "batch": B, "parallelism": f"replicas x{dist.world}",
                        "l2": f"inputs {in_bytes / 1e6:.0f} MB per rank > 126 MB L2 (no flush needed)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         # DRAM read + write bytes of one launch: an ncu capture of this
+                         # kernel on the 256-instance case (--profile-small) read 1.857536 MB
+                         # and wrote 0 B; scaled by the instances per launch (each matrix is
+                         # read once, so DRAM traffic grows in proportion)
+                         "traffic": 1.857536e6 / 256 * B,
+                         "traffic_unit": "bytes per launch (ncu capture scaled by instances)",
                          "peak_source": "FP64 mma.m16n8k8 throughput measured live (gbs_probe_fp64_peak); "
                                         "MEASURED_PEAKS.json has no FP64 figure",
                          "flops_per_step": algo_flops,

@@ -298,7 +298,13 @@ def tor_batched(matrices: Iterable[Any], precision: str = "fp64", backend: str =
 
 def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: bool = False):
     """Single large torontonian of a real (2n, 2n) matrix, 2n <= 64
-    (gbskernels/__init__.py:635-691 contract)."""
+    (gbskernels/__init__.py:635-691 contract).
+
+    One instance split into at least ``2**groups`` prefix work items over the
+    whole GPU (the warp-cooperative walk of the batched kernel, lifted to 32
+    modes).  ``certified=True`` returns ``(value, diagnostics)`` with a rigorous
+    a-posteriori bound; ``dd=True`` (the reference's double-double certified
+    variant) is not provided and raises RuntimeError."""
     A = np.asarray(O)
     if np.iscomplexobj(A):
         if np.any(np.imag(A) != 0):
@@ -320,9 +326,14 @@ def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: b
     lib = _lib.load()
     v = np.zeros(1)
     e = np.zeros(1)
-    if certified or dd:
-        tier = "certified-dd" if dd else "certified-fp64"
-        name = "gbs_tor_single_ddcertified_host" if dd else "gbs_tor_single_certified_host"
+    if dd:
+        # the reference's double-double certified single-large kernel has no
+        # counterpart here; like the reference without it, this is a RuntimeError
+        raise RuntimeError("tor_single(certified-dd) is not in this build; use certified=True "
+                           "(binary64 value with a rigorous a-posteriori bound)")
+    if certified:
+        tier = "certified-fp64"
+        name = "gbs_tor_single_certified_host"
         fn = getattr(lib, name, None)
         if fn is None:
             raise RuntimeError(f"tor_single({tier}) is not in this build")

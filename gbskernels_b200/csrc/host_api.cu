@@ -86,7 +86,8 @@ static unsigned cover(unsigned need) {
 // ------------------------------------------------------------------ caps
 constexpr int kPermCap = 28;
 constexpr int kHafCap = kHafMaxN;   // 32 (after odd-N loop augmentation)
-constexpr int kTorCapModes = 24;
+constexpr int kTorCapModes = 24;        // batched torontonian
+constexpr int kTorSingleCapModes = 32;  // single-large torontonian (binary64 tiers)
 
 // ------------------------------------------------------------------ requests and plans
 struct Req {
@@ -100,6 +101,10 @@ struct Req {
   const int* idx = nullptr;       // host, dim indices
   int M = 0;
   int state_real = 0;
+  // single-large torontonian: the 32-mode cap applies, and the prefix split is at
+  // least 2^split work items (the reference's `groups`)
+  int single = 0;
+  int split = -1;
 };
 
 // Device gather of resident-state submatrices (k_gather.cu).
@@ -145,7 +150,7 @@ static double item_cost(int fn, int dim, unsigned long long count, int tier, int
 }
 
 // Append one instance (already validated) to the plan.  Returns the instance index.
-static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, long long off) {
+static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, long long off, int split = -1) {
   InstDesc d{};
   d.off = off;
   d.dim = dim_eval;
@@ -190,9 +195,10 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
   } else {  // tor, binary64 tiers: one warp per prefix pattern over the first g prefix modes
     const int n = dim_eval / 2;
     const int q = n - std::min(n, 5);
-    // 2^9 leaves (x 32 tail subsets) per item; 2^10 for the certified tier, whose
-    // items also repeat the per-instance eigenvalue proof
-    const int g = std::max(0, q - (tier == kTierCert ? 10 : 9));
+    // 2^9 leaves (x 32 tail subsets) per item, the same split for every binary64
+    // tier so that the certified and indicator values are the fp64 value bit for bit
+    int g = std::max(0, q - 9);
+    if (split >= 0) g = std::min(q, std::max(g, split));
     for (unsigned long long p = 0; p < (1ull << g); ++p) add(p, 1);
     d.param = g;
   }
@@ -323,7 +329,13 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
     case kFnTor: {
       if (r.dim & 1) return fail(cudaErrorInvalidValue, "torontonian: matrix side must be even");
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
-      if (r.dim / 2 > kTorCapModes) return fail(cudaErrorInvalidValue, "torontonian: modes above the cap 24");
+      if (r.single) {
+        if (r.tier == kTierDD) return fail(cudaErrorNotSupported, "single-large torontonian: no double-double tier");
+        if (r.dim / 2 > kTorSingleCapModes)
+          return fail(cudaErrorInvalidValue, "single-large torontonian: modes above the cap 32");
+      } else if (r.dim / 2 > kTorCapModes) {
+        return fail(cudaErrorInvalidValue, "torontonian: modes above the cap 24");
+      }
       bool re = true;
       if (r.state) {
         re = r.state_real != 0;
@@ -413,7 +425,7 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
   size_t meta_bytes = 0, tot_items = 0, tot_inst = 0;
   for (size_t g = 0; g < plans.size(); ++g) {
     Plan& P = plans[g];
-    for (int i : greq[g]) plan_instance(P, reqs[i].fn, reqs[i].tier, dim_eval[i], real_in[i], off[i]);
+    for (int i : greq[g]) plan_instance(P, reqs[i].fn, reqs[i].tier, dim_eval[i], real_in[i], off[i], reqs[i].split);
     P.ws_doubles = ws_for_plan(P);
     const int ni = (int)P.insts.size(), nit = (int)P.items.size();
     std::vector<int> inst_order(ni);
@@ -793,6 +805,50 @@ int gbs_perm_certified_host(const double* m, int n, int b, double* o, double* e)
 int gbs_haf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnHaf, m, N, b, o, e); }
 int gbs_lhaf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnLhaf, m, N, b, o, e); }
 int gbs_tor_certified_host(const double* m, int n, int b, double* o, double* e) { return one_shot_cert(kFnTor, m, 2 * n, b, o, e); }
+
+// ---- single-large torontonian (core/host_api.cu:270-352) ---------------------
+// Real (2n x 2n) O, n <= 32, evaluated as ONE instance split into at least 2^g
+// prefix work items over the whole GPU.  Off the physical domain the value is NaN
+// (and the bound +inf); the certified variant returns the a-posteriori bound.
+static int tor_single(int tier, const double* O, int n, int g, double* out, double* bound) {
+  if (!O || !out || (tier == kTierCert && !bound)) return fail(cudaErrorInvalidValue, "null pointer");
+  if (n < 0 || n > kTorSingleCapModes) return fail(cudaErrorInvalidValue, "single-large torontonian: n must be in [0, 32]");
+  if (g < 0 || g > n) return fail(cudaErrorInvalidValue, "single-large torontonian: groups must be in [0, n]");
+  const int dim = 2 * n;
+  std::vector<double> c(2 * (size_t)dim * dim, 0.0);
+  for (size_t i = 0; i < (size_t)dim * dim; ++i) {
+    if (!std::isfinite(O[i])) return fail(cudaErrorInvalidValue, "single-large torontonian: non-finite input");
+    c[2 * i] = O[i];
+  }
+  gbs_session* s;
+  int rc = with_default(&s);
+  if (rc) return rc;
+  Req r{};
+  r.fn = kFnTor;
+  r.tier = tier;
+  r.dim = dim;
+  r.mat = c.data();
+  r.single = 1;
+  r.split = g;
+  double o[2] = {0.0, 0.0}, aux = 0.0;
+  int st = 0;
+  RunOpts opt;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    rc = run_batch(s, std::vector<Req>{r}, o, &aux, &st, opt);
+  }
+  if (rc) return rc;
+  const bool ok = st == kStOk && std::isfinite(o[0]);
+  *out = ok ? o[0] : NAN;
+  if (bound) *bound = ok ? aux : INFINITY;
+  return 0;
+}
+int gbs_tor_recursive_single_host(const double* O, int n, int g, double* out) {
+  return tor_single(kTierFp64, O, n, g, out, nullptr);
+}
+int gbs_tor_single_certified_host(const double* O, int n, int g, double* out, double* bound) {
+  return tor_single(kTierCert, O, n, g, out, bound);
+}
 
 // ---- auto tier on the device (gbskernels/__init__.py:272-297) ----------------
 // func: 0 perm, 1 haf, 2 lhaf, 3 tor; dim = matrix side.  tier_out: 0 fp64, 1 dd.

@@ -29,17 +29,25 @@
 //   * the factor, Zd and the pivot reciprocals live in the warp's shared workspace
 //     (about 18 KB at 24 modes): no local memory.
 //
+// Pivots: the factor keeps 1 / L[j][j] = rsqrt(s_j) (s_j the pivot before the root);
+// off-diagonal entries are s_ij * rsqrt(s_j), det = prod s_j, term = rsqrt(det).
+// CUDA documents double rsqrt to 1 ulp; the certified bound below assumes 2 ulp
+// (relative error <= 4u), so it does not lean on the last ulp of that figure.
+//
 // Certified tier: the binary64 walk is the fp64 tier's (bit-identical value) and each
-// term gets an a-posteriori radius.  For a subset of dimension m the computed factor
-// satisfies L^L^T = A + F with |F_ij| <= c_m D_i D_j (Cholesky backward error,
-// gamma_{m+2}, reciprocal-multiply counted; D_i = fl(sqrt(fl(1 - O_ii)))), so
-// det(L^)^2 = det(A) det(I + X) with ||X|| <= eta_m = m c_m / sigma, sigma a rigorous
-// lower bound of lambda_min(D^-1 M D^-1) -- valid for every principal submatrix by
-// Cauchy interlacing, so ONE bound per instance certifies all 2^k subsets.  sigma is
-// proved per instance by a binary64 Cholesky of D^-1 M D^-1 - sigma I that succeeds
-// (success implies lambda_min >= -gamma_{m+2} tr / (1 - gamma_{m+2}), Weyl for the
-// rounding of the scaled matrix).  The term radius is |t^| rho_m with rho_m from the
-// eta_m, pivot-product and final sqrt / division roundings (tor_cert_rho).
+// term gets an a-posteriori radius.  Define L^_jj := 1 / rsqrt(s_j) (exact real).  For
+// a subset of dimension m the computed factor then satisfies L^L^T = A + F with
+// |F_ij| <= c_m D_i D_j (Cholesky backward error: each entry is an inner product of
+// <= m fused terms and one scaling, the diagonal carries (1 + 4u)^2 from rsqrt, so
+// gamma_{m+10} covers it; D_i = fl(sqrt(fl(1 - O_ii)))), hence det(L^)^2 =
+// det(A) det(I + X) with ||X|| <= eta_m = m c_m / sigma, sigma a rigorous lower bound
+// of lambda_min(D^-1 M D^-1) -- valid for every principal submatrix by Cauchy
+// interlacing, so ONE bound per instance certifies all 2^k subsets.  sigma is proved
+// per instance by a binary64 Cholesky of D^-1 M D^-1 - sigma I that succeeds (success
+// implies lambda_min >= -g tr / (1 - g), g = gamma_{2k+10}; Weyl for the rounding of
+// the scaled matrix), at a sigma guessed by inverse iteration.  The term radius is
+// |t^| rho_m with rho_m from eta_m, the pivot product (m + 1 roundings), the rsqrt
+// of every pivot and the final rsqrt (tor_cert_rho).
 #pragma once
 
 #include "cert.cuh"
@@ -69,8 +77,8 @@ __host__ __device__ inline TorWLayout tor_w_layout(int kmax, bool cert) {
   Lw.gidx_off = Lw.det_off + q + 2;
   Lw.rho_off = Lw.gidx_off + (rows + 2) / 2;
   int total = Lw.rho_off + (cert ? 2 * kmax + 2 : 0);
-  if (cert) {  // the sigma proof factors a packed 2k x 2k matrix in the col / zd region
-    const int need = (2 * kmax) * (2 * kmax + 1) / 2 + 8;
+  if (cert) {  // the sigma proof factors a packed 2k x 2k matrix (+ 2k scalings) in the col / zd region
+    const int need = (2 * kmax) * (2 * kmax + 1) / 2 + 2 * kmax + 8;
     if (Lw.det_off < need) {
       const int shift = need - Lw.det_off;
       Lw.det_off += shift;
@@ -116,13 +124,18 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
     gidx[R0] = gR0;
     gidx[R1] = gR1;
   }
-  // residual slots x = lane, lane + 32
+  // residual slots x = lane, lane + 32: kind 1 = prefix column x (read L[x][v] at
+  // column offset x - v while x > v), 2 / 3 = the new diagonal slots, 4 = tail column
+  // (read W[v][jt] at offset rows + jt - v), 0 = idle
   double a[2], b[2];
+  int kind[2], off[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int x = lane + 32 * h;
     a[h] = 0.0;
     b[h] = 0.0;
+    kind[h] = x < R0 ? 1 : x == R0 ? 2 : x == R1 ? 3 : x < nx ? 4 : 0;
+    off[h] = kind[h] == 1 ? x : rows + (x - R0 - 2);
     if (x < R0) {
       const int gc = gidx[x];
       a[h] = tor_m(Oc, dim, gR0, gc);
@@ -142,38 +155,22 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
   for (int v = 0; v < R0; ++v) {
     const int owner = v & 31;
     double* cv = col + tor_col_base(v, rows);
-    double l0 = 0.0, l1 = 0.0;
+    // the owner's finished residual, broadcast; every lane scales it (same value)
+    const double iv = inv[v];
+    const double l0 = __shfl_sync(0xffffffffu, (v >> 5) ? a[1] : a[0], owner) * iv;
+    const double l1 = __shfl_sync(0xffffffffu, (v >> 5) ? b[1] : b[0], owner) * iv;
     if (lane == owner) {
-      const double iv = inv[v];
-      l0 = ((v >> 5) ? a[1] : a[0]) * iv;
-      l1 = ((v >> 5) ? b[1] : b[0]) * iv;
       cv[R0 - v] = l0;
       cv[R1 - v] = l1;
     }
-    l0 = __shfl_sync(0xffffffffu, l0, owner);
-    l1 = __shfl_sync(0xffffffffu, l1, owner);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int x = lane + 32 * h;
-      double e;
-      bool upd = true;
-      if (x < R0) {
-        upd = x > v;
-        e = upd ? cv[x - v] : 0.0;
-      } else if (x == R0) {
-        e = l0;
-      } else if (x == R1) {
-        e = l1;
-      } else if (x < nx) {
-        e = cv[rows - v + (x - R0 - 2)];
-      } else {
-        upd = false;
-        e = 0.0;
-      }
-      if (upd) {
-        a[h] = fma(-e, l0, a[h]);
-        b[h] = fma(-e, l1, b[h]);
-      }
+      double e = 0.0;  // 0 for finished or idle slots: fma(-0, l, a) == a
+      if ((kind[h] == 1 && x > v) || kind[h] == 4) e = cv[off[h] - v];
+      e = kind[h] == 2 ? l0 : (kind[h] == 3 ? l1 : e);
+      a[h] = fma(-e, l0, a[h]);
+      b[h] = fma(-e, l1, b[h]);
     }
   }
   // the two diagonal slots
@@ -183,14 +180,14 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
   const double m10 = __shfl_sync(0xffffffffu, h0 ? b[1] : b[0], o0);
   bool ok = s0 > 0.0;
   if (!ok) s0 = 1.0;
-  const double i0 = 1.0 / sqrt(s0);
+  const double i0 = rsqrt(s0);
   const double l10 = m10 * i0;
   double s1 = fma(-l10, l10, __shfl_sync(0xffffffffu, h1 ? b[1] : b[0], o1));
   if (!(s1 > 0.0)) {
     ok = false;
     s1 = 1.0;
   }
-  const double i1 = 1.0 / sqrt(s1);
+  const double i1 = rsqrt(s1);
   double* c0 = col + tor_col_base(R0, rows);
   double* c1 = col + tor_col_base(R1, rows);
 #pragma unroll
@@ -243,8 +240,8 @@ __device__ __forceinline__ double tor_w_leaf(const double* zc, int r, int c, int
   m = 0;
   if (lane < (1 << r)) {
     const int td = 2 * r;
-    double Lz[kTorZE];
-    double iv[kTorTD];
+    double Lz[kTorZE];  // off-diagonal entries (the diagonal slots stay unused)
+    double iv[kTorTD];  // 1 / L[i][i]
     double det = 1.0;
 #pragma unroll
     for (int i = 0; i < kTorTD; ++i) {
@@ -263,16 +260,14 @@ __device__ __forceinline__ double tor_w_leaf(const double* zc, int r, int c, int
             ok = false;
             s = 1.0;
           }
-          const double d = sqrt(s);
-          Lz[e] = d;
-          iv[i] = 1.0 / d;
+          iv[i] = in_i ? rsqrt(s) : 1.0;  // excluded rows: s == 1 exactly
           det *= s;
         }
       }
     }
     const int nin = __popc(lane);
     m = 2 * (c + nin);
-    const double t = 1.0 / sqrt(detc * det);
+    const double t = rsqrt(detc * det);
     term = ((k - c - nin) & 1) ? -t : t;
   }
   return term;
@@ -281,37 +276,41 @@ __device__ __forceinline__ double tor_w_leaf(const double* zc, int r, int c, int
 // ------------------------------------------------------------ certified prologue
 // Rigorous lower bound sigma of lambda_min(D^-1 M D^-1), D_i = fl(sqrt(fl(1 - O_ii))),
 // for the whole 2k x 2k matrix; <= 0 when none could be proved.  Also returns a lower
-// bound of min D_i^2 for the underflow term.  Scratch: packed lower (2k)(2k+1)/2
-// doubles at S (warp-private shared memory).
-static __device__ double tor_cert_sigma(const double* __restrict__ Oc, int k, double* S, int lane, double& dmin2) {
+// bound of min D_i^2 for the underflow term.  Scratch (warp-private shared memory):
+// the packed lower (2k)(2k+1)/2 matrix at S, then 2k scalings.
+//   H^_ij = fl(fl(m_ij * fl(1/D_i)) * fl(1/D_j)) is within gamma_5 |h_ij| of the exact
+//   scaled entry, so ||H^ - H||_2 <= ||H^ - H||_F <= gamma_5 / (1 - gamma_5) ||H^||_F.
+//   A binary64 Cholesky of B = fl(H^ - s I) that completes proves lambda_min(B) >=
+//   -g tr(B) / (1 - g), g = gamma_{2k+10} (backward error of the factorisation, the
+//   rsqrt pivots included); with the rounding of the diagonal shift (u sum |b_ii|),
+//   lambda_min(H) >= s - g tr / (1 - g) - ||E||.
+//   The trial shift comes from inverse iteration with the factor of H^ itself.
+static __device__ __noinline__ double tor_cert_sigma(const double* __restrict__ Oc, int k, double* S, int lane, double& dmin2) {
   const int dim = 2 * k;
   const int np = dim * (dim + 1) / 2;
+  double* dinv = S + np;
   double dm = 1e300;
   bool okd = true;
   for (int i = lane; i < dim; i += 32) {
     const double mii = 1.0 - Oc[2 * (i * dim + i)];
     if (!(mii > 0.0)) okd = false;
-    const double di = mii > 0.0 ? sqrt(mii) : 0.0;
+    const double di = mii > 0.0 ? sqrt(mii) : 1.0;
+    dinv[i] = 1.0 / di;
     dm = fmin(dm, __dmul_rd(di, di));
   }
   okd = __all_sync(0xffffffffu, okd);
 #pragma unroll
   for (int mm = 16; mm > 0; mm >>= 1) dm = fmin(dm, shfl_xor_d(dm, mm));
   dmin2 = dm;
+  __syncwarp();
   if (!okd) return -1.0;
-  auto hval = [&](int i, int jj) {
-    const double di = sqrt(1.0 - Oc[2 * (i * dim + i)]);
-    const double dj = sqrt(1.0 - Oc[2 * (jj * dim + jj)]);
-    return tor_m(Oc, dim, i, jj) / di / dj;
-  };
   auto unpack = [&](int e, int& i, int& jj) {
     i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
     while (i * (i + 1) / 2 > e) --i;
     while ((i + 1) * (i + 2) / 2 <= e) ++i;
     jj = e - i * (i + 1) / 2;
   };
-  // ||H^||_F (upward); H^ = fl(fl(m_ij / D_i) / D_j) is within gamma_3 |h| of the
-  // exact scaled entry, so ||E_H||_F <= gamma_3 / (1 - gamma_3) ||H^||_F
+  auto hval = [&](int i, int jj) { return (tor_m(Oc, dim, i, jj) * dinv[i]) * dinv[jj]; };
   double fro2 = 0.0;
   for (int e = lane; e < np; e += 32) {
     int i, jj;
@@ -321,11 +320,12 @@ static __device__ double tor_cert_sigma(const double* __restrict__ Oc, int k, do
     if (i != jj) fro2 = ru_fma(h, h, fro2);
   }
   fro2 = warp_sum_ru(fro2);
-  const double g3 = gamma_ru(3.0, kU);
-  const double eh = ru_mul(ru_div(g3, rd_sub(1.0, g3)), ru_sqrt(fro2));
-  const double gm = gamma_ru((double)(dim + 2), kU);
-  // one attempt: factor B = fl(H^ - sig I) in place (right-looking, packed lower);
-  // on success return the proved bound sig - tau - ||E||, else -1
+  const double g5 = gamma_ru(5.0, kU);
+  const double eh = ru_mul(ru_div(g5, rd_sub(1.0, g5)), ru_sqrt(fro2));
+  const double gm = gamma_ru((double)(dim + 10), kU);
+  // factor B = fl(H^ - sig I) in place (right-looking, packed lower; the diagonal
+  // slot of column j ends holding rsqrt of its pivot); on success return the proved
+  // bound sig - tau - ||E||, else -1
   auto attempt = [&](double sig) -> double {
     double trace = 0.0;
     for (int e = lane; e < np; e += 32) {
@@ -346,8 +346,9 @@ static __device__ double tor_cert_sigma(const double* __restrict__ Oc, int k, do
         __syncwarp();
         return -1.0;
       }
-      const double id = 1.0 / sqrt(p);
+      const double id = rsqrt(p);
       __syncwarp();
+      if (lane == 0) S[jc * (jc + 1) / 2 + jc] = id;
       for (int i = jc + 1 + lane; i < dim; i += 32) S[i * (i + 1) / 2 + jc] *= id;
       __syncwarp();
       for (int i = jc + 1; i < dim; ++i) {
@@ -357,48 +358,61 @@ static __device__ double tor_cert_sigma(const double* __restrict__ Oc, int k, do
       }
       __syncwarp();
     }
-    // success: lambda_min(B) >= -tau, tau = gm tr(B) / (1 - gm); the distance of B to
-    // the exact H - sig I is at most eh + u sum |b_ii| (rounding of the diagonal shift)
     const double tau = ru_div(ru_mul(gm, trace), rd_sub(1.0, gm));
     const double err = ru_add(eh, ru_mul(kUc, trace));
     return rd_sub(rd_sub(sig, tau), err);
   };
-  // halve sig from 1/2 until a factorisation succeeds, then three bisection steps
-  double best = -1.0, sig = 0.5, fail_at = 1.0;
-  for (int t = 0; t < 40 && best <= 0.0; ++t) {
-    const double c = attempt(sig);
-    if (c > 0.0) {
-      best = c;
-    } else {
-      fail_at = sig;
-      sig *= 0.5;
+  if (attempt(0.0) < -0.5) return -1.0;  // H^ itself does not factor
+  // inverse iteration x <- (L L^T)^{-1} x with the factor in S (slots x = lane, lane + 32)
+  double x0 = lane < dim ? 1.0 + 0.01 * lane : 0.0;
+  double x1 = lane + 32 < dim ? 1.0 + 0.01 * (lane + 32) : 0.0;
+  double mu = 1.0;
+  for (int it = 0; it < 5; ++it) {
+    for (int j = 0; j < dim; ++j) {  // L y = x
+      const double yj = __shfl_sync(0xffffffffu, (j >> 5) ? x1 : x0, j & 31) * S[j * (j + 1) / 2 + j];
+      if (lane == (j & 31)) {
+        if (j >> 5) x1 = yj;
+        else x0 = yj;
+      }
+      if (lane > j && lane < dim) x0 = fma(-S[lane * (lane + 1) / 2 + j], yj, x0);
+      if (lane + 32 > j && lane + 32 < dim) x1 = fma(-S[(lane + 32) * (lane + 33) / 2 + j], yj, x1);
     }
-  }
-  if (best <= 0.0) return -1.0;
-  double lo = sig, hi = fail_at;
-  for (int b = 0; b < 3; ++b) {
-    const double mid = 0.5 * (lo + hi);
-    const double c = attempt(mid);
-    if (c > 0.0) {
-      lo = mid;
-      best = fmax(best, c);
-    } else {
-      hi = mid;
+    for (int j = dim - 1; j >= 0; --j) {  // L^T z = y
+      const double zj = __shfl_sync(0xffffffffu, (j >> 5) ? x1 : x0, j & 31) * S[j * (j + 1) / 2 + j];
+      if (lane == (j & 31)) {
+        if (j >> 5) x1 = zj;
+        else x0 = zj;
+      }
+      const int r0 = j * (j + 1) / 2;
+      if (lane < j) x0 = fma(-S[r0 + lane], zj, x0);
+      if (lane + 32 < j) x1 = fma(-S[r0 + lane + 32], zj, x1);
     }
+    double nn = x0 * x0 + x1 * x1;
+#pragma unroll
+    for (int mm = 16; mm > 0; mm >>= 1) nn += shfl_xor_d(nn, mm);
+    mu = sqrt(nn);  // ~ 1 / lambda_min once converged (x had unit norm)
+    if (!(mu > 0.0) || !isfinite(mu)) return -1.0;
+    x0 /= mu;
+    x1 /= mu;
   }
+  const double est = 1.0 / mu;  // >= lambda_min(H^) up to rounding
+  double best = -1.0;
+  const double fr[6] = {0.9, 0.7, 0.45, 0.2, 0.05, 0.01};
+  for (int t = 0; t < 6 && best <= 0.0; ++t) best = attempt(fr[t] * est);
   return best;
 }
 
 // rho_m for m = 0..2k (a-posteriori relative radius of one term of dimension m),
-// written to rho[]; +inf where m * eta_m is not below 1/2.
-//   c_m   = (g/(1-g) + u/(1-u)) / (1-u)^2 + (m+2) ufl / dmin2,  g = gamma_{m+2}
-//   eta_m = m c_m / sigma
-//   t / t^ lies in [Lo, Up] with
-//   Up = sqrt((1 + gamma_{m+1}) / ((1 - m eta)(1 - 2mu))) (1+u)/(1-u)
-//   Lo = sqrt((1 - gamma_{m+1})(1 - m eta)(1 - 2mu)) (1-u)/(1+u)
-// (pivot product: m+1 roundings; fl(sqrt) of each pivot squared: (1 +- u)^{2m};
-// det(I + X) within (1 -+ eta)^m; the final sqrt and division), rho = max(Up-1, 1-Lo).
-static __device__ void tor_cert_rho(double sigma, double dmin2, int k, double* rho, int lane) {
+// written to rho[]; +inf where m * eta_m is not below 1/2.  e_r = 4u bounds the
+// relative error of rsqrt (2 ulp).
+//   c_m   = (g/(1-g) + u/(1-u)) / (1-u)^2 + (m+10) ufl / dmin2,  g = gamma_{m+10}
+//   eta_m = m c_m / sigma,   gp = gamma_{m+1} (pivot product)
+//   t / t^ = sqrt(det(I+X) (1+theta_p)) prod_j (1+d_j) / (1+d_f), |d| <= e_r, so
+//   Up = sqrt((1+gp) / (1 - m eta)) / ((1 - m e_r)(1 - e_r))
+//   Lo = sqrt((1-gp)(1 - m eta)) (1 - m e_r) / (1 + e_r)
+//   and rho = max(Up - 1, 1 - Lo) bounds |t - t^| / |t^|.
+static __device__ __noinline__ void tor_cert_rho(double sigma, double dmin2, int k, double* rho, int lane) {
+  const double er = 4.0 * kU;
   for (int m = lane; m <= 2 * k; m += 32) {
     double out;
     if (m == 0) {
@@ -407,22 +421,23 @@ static __device__ void tor_cert_rho(double sigma, double dmin2, int k, double* r
       out = INFINITY;
     } else {
       const double md = (double)m;
-      const double g = gamma_ru(md + 2.0, kU);
+      const double g = gamma_ru(md + 10.0, kU);
       double cm = ru_add(ru_div(g, rd_sub(1.0, g)), ru_div(kU, rd_sub(1.0, kU)));
       cm = ru_div(cm, __dmul_rd(rd_sub(1.0, kU), rd_sub(1.0, kU)));
-      cm = ru_add(cm, ru_div(ru_mul(md + 2.0, kUfl), dmin2));
+      cm = ru_add(cm, ru_div(ru_mul(md + 10.0, kUfl), dmin2));
       const double eta = ru_div(ru_mul(md, cm), sigma);
       const double meta = ru_mul(md, eta);
-      if (!(meta < 0.5)) {
+      const double mer = ru_mul(md, er);
+      if (!(meta < 0.5) || !(mer < 0.5)) {
         out = INFINITY;
       } else {
         const double gp = gamma_ru(md + 1.0, kU);
-        const double two_mu = ru_mul(2.0 * md, kU);
-        const double den = __dmul_rd(rd_sub(1.0, meta), rd_sub(1.0, two_mu));
-        double up = ru_sqrt(ru_div(ru_add(1.0, gp), den));
-        up = ru_div(ru_mul(up, ru_add(1.0, kU)), rd_sub(1.0, kU));
-        double lo = rd_sqrt(__dmul_rd(rd_sub(1.0, gp), den));
-        lo = __ddiv_rd(__dmul_rd(lo, rd_sub(1.0, kU)), ru_add(1.0, kU));
+        const double one_meta = rd_sub(1.0, meta);
+        const double one_mer = rd_sub(1.0, mer);
+        double up = ru_sqrt(ru_div(ru_add(1.0, gp), one_meta));
+        up = ru_div(up, __dmul_rd(one_mer, rd_sub(1.0, er)));
+        double lo = rd_sqrt(__dmul_rd(rd_sub(1.0, gp), one_meta));
+        lo = __ddiv_rd(__dmul_rd(lo, one_mer), ru_add(1.0, er));
         out = fmax(ru_add(up, -1.0), ru_add(1.0, -lo));
       }
     }

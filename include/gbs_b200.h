@@ -59,6 +59,18 @@ int gbs_haf_certified_host(const double* mats, int N, int batch, double* out, do
 int gbs_lhaf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
 int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, double* bound);
 
+/* ---- single-large torontonian ----------------------------------------------
+ * reference: core/host_api.cu:270-298 (gbs_tor_recursive_single_host) and :300-352
+ * (gbs_tor_single_certified_host); bindings/gbskernels_ext.cpp:46-47.
+ * O: real (2n x 2n) row-major binary64 (NOT complex), n <= 32.  One torontonian
+ * split into at least 2^g prefix work items across the GPU (g in [0, n], the
+ * reference's `groups`; the planner may split further).  Off the physical domain
+ * (a non-SPD minor of I - O) *out is NaN and *bound +inf.  The certified bound is
+ * rigorous: |*out - tor(O)| <= *bound.  The reference's double-double certified
+ * single-large variant (gbs_tor_single_ddcertified_host) is not provided.        */
+int gbs_tor_recursive_single_host(const double* O, int n, int g, double* out);
+int gbs_tor_single_certified_host(const double* O, int n, int g, double* out, double* bound);
+
 /* ---- auto tier on the device ----------------------------------------------
  * reference: gbskernels/__init__.py:272-297 (_gpu_auto_batched) whose fp64 pass is
  * gbs_*_kappa_host and whose rerun is gbs_*_dd_host; here both run in the library.

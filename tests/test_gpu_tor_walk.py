@@ -34,18 +34,21 @@ def test_tor_sizes_vs_binary128(gpu, orc, n):
     mats = np.stack([phys_O(n), phys_O(n, 3.0)])
     truth = [orc.tor(m, "quad") for m in mats]
     fp = gpu.tor_batched(mats)
+    _, diag = gpu.tor_batched(mats, precision="auto", return_diagnostics=True)
     cv, cb = _cert(gpu, mats)
     assert np.array_equal(cv, fp)  # the certified value is the binary64 value
     for i in range(2):
-        assert rel_err(fp[i], truth[i]) < 1e-12, (n, i)
+        # sum |term| / |tor| grows like 3^n here: the binary64 error scales with it
+        kappa = diag[i]["cancellation"]
+        assert rel_err(fp[i], truth[i]) < max(1e-13, 1e-15 * kappa), (n, i, kappa)
         assert abs(cv[i] - truth[i]) <= cb[i], (n, i, abs(cv[i] - truth[i]), cb[i])
-        assert cb[i] <= 1e-9 * abs(truth[i]), (n, i, cb[i] / abs(truth[i]))
+        assert cb[i] <= 1e-9 * kappa * abs(truth[i]), (n, i, cb[i] / abs(truth[i]), kappa)
 
 
 @pytest.mark.parametrize("n", [14, 15, 16, 17])
 def test_tor_multi_item_vs_dd_kernel(gpu, n):
-    # 14: one item in both decompositions; 15/16/17: 2/4/8 items (binary64) and
-    # 1/2/4 items (certified).  The double-double kernel is a separate code path.
+    # 14: one work item; 15/16/17: 2/4/8 items (every binary64 tier splits the same
+    # way).  The double-double kernel is a separate code path.
     mats = np.stack([phys_O(n) for _ in range(2)])
     _, diag = gpu.tor_batched(mats, precision="auto", return_diagnostics=True)
     dd = gpu.tor_batched(mats, precision="dd")
@@ -56,7 +59,7 @@ def test_tor_multi_item_vs_dd_kernel(gpu, n):
         kappa = diag[i]["cancellation"]
         assert rel_err(f64[i], dd[i]) < max(1e-12, 1e-15 * kappa), (n, i, kappa)
         assert abs(cv[i] - dd[i]) <= cb[i], (n, i)
-        assert cb[i] <= 1e-8 * abs(dd[i]), (n, i, cb[i] / abs(dd[i]))
+        assert cb[i] <= 1e-9 * kappa * abs(dd[i]), (n, i, cb[i] / abs(dd[i]), kappa)
 
 
 def test_tor_ragged_batch_equals_alone(gpu):
