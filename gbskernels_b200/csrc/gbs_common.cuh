@@ -218,6 +218,16 @@ __device__ __forceinline__ void dmma_m16n8k4(double (&d)[4], double a0, double a
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// D += A B with m16n8k8 (A: rows g / g+8, columns t4 / t4+4; B: rows t4 / t4+4,
+// column g): the work of two consecutive m16n8k4 steps in one instruction.
+__device__ __forceinline__ void dmma_m16n8k8(double (&d)[4], double a0, double a1, double a2, double a3, double b0,
+                                             double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 // 16-byte complex loads / stores (shared or global memory, 16-byte aligned).
 __device__ __forceinline__ cplx ld_c(const double* p) {
   double2 v = *reinterpret_cast<const double2*>(p);

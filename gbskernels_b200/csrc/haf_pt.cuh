@@ -1,5 +1,5 @@
 // haf_pt.cuh -- hafnian and loop hafnian by the power-trace formula, one warp per
-// subset, binary64 on the FP64 tensor cores (mma.sync .m16n8k4 .f64).
+// subset, binary64 on the FP64 tensor cores (mma.sync .m16n8k8 / .m16n8k4 .f64).
 //
 // Algorithm (the reference's, cpu_ref/hafnian.py:101-129 and
 // cpu_ref/loop_hafnian.py:65-108; device form core/hafnian.cu:41-133,
@@ -15,10 +15,10 @@
 //     staged in shared memory.
 //   * All 16-row strips of C^a advance together: C^{a+1} = C^a C on the FP64 tensor
 //     cores through the real embedding [Re P, Im P] (interleaved) x B',
-//     B'[2k+p][2j+q] = (p ? iC : C)[k][j] component (q ? im : re): one m16n8k4 mma
-//     consumes two complex columns; each B' fragment is loaded once and used by
-//     every strip; with few tiles the K loop is split into two accumulator sets so
-//     at least eight independent mma chains are in flight.
+//     B'[2k+p][2j+q] = (p ? iC : C)[k][j] component (q ? im : re): one m16n8k8 mma
+//     consumes four complex columns (an m16n8k4 finishes an odd count); each B'
+//     fragment is loaded once and used by every strip; with few tiles the K loop is
+//     split into two accumulator sets so more independent mma chains are in flight.
 //   * Since C^T = X C X (B_S symmetric), (C^a)^T = X C^a X and
 //       tr(C^{2a})   = sum_{i,t} C^a[i][t]     C^a[i^1][t^1]
 //       tr(C^{2a-1}) = sum_{i,t} C^a[i][t] C^{a-1}[i^1][t^1],
@@ -108,8 +108,33 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
   const double* bptr = Cs + ((t4 >> 1) * cs + (g >> 1)) * 2 + ((t4 ^ g) & 1);
   const unsigned long long sgn = ((t4 & 1) && !(g & 1)) ? 0x8000000000000000ull : 0ull;
   const double* ap = P + g * ps * 2 + t4;
-  const int ksn = s >> 1;  // K = 2s real columns, 4 per slice
-  auto slice = [&](int ks, int k2) {
+  const int ksn = s >> 1;  // K = 2s real columns: ksn slices of 4, paired into m16n8k8 steps
+  // k8 step j = k4 slices 2j (A columns t4, B' rows t4) and 2j + 1 (A columns t4 + 4,
+  // B' rows t4 + 4)
+  auto step8 = [&](int j, int k2) {
+    const int k0 = 2 * j, k1 = 2 * j + 1;
+    double a0[MS], a1[MS], a2[MS], a3[MS];
+#pragma unroll
+    for (int ms = 0; ms < MS; ++ms) {
+      a0[ms] = ap[(16 * ms) * ps * 2 + 4 * k0];
+      a1[ms] = ap[(16 * ms + 8) * ps * 2 + 4 * k0];
+      a2[ms] = ap[(16 * ms) * ps * 2 + 4 * k1];
+      a3[ms] = ap[(16 * ms + 8) * ps * 2 + 4 * k1];
+    }
+    const double* bp0 = bptr + k0 * 4 * cs;
+    const double* bp1 = bptr + k1 * 4 * cs;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      if (nt < ntn) {
+        const double b0 = __longlong_as_double(__double_as_longlong(bp0[nt * 8]) ^ sgn);
+        const double b1 = __longlong_as_double(__double_as_longlong(bp1[nt * 8]) ^ sgn);
+#pragma unroll
+        for (int ms = 0; ms < MS; ++ms) dmma_m16n8k8(acc[k2][ms][nt], a0[ms], a1[ms], a2[ms], a3[ms], b0, b1);
+      }
+    }
+  };
+  // a trailing single k4 slice when ksn is odd
+  auto step4 = [&](int ks, int k2) {
     double a0[MS], a1[MS];
 #pragma unroll
     for (int ms = 0; ms < MS; ++ms) {
@@ -126,14 +151,16 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
       }
     }
   };
+  const int n8 = ksn >> 1;
   if constexpr (KS2 == 2) {
-    int ks = 0;
+    int j = 0;
 #pragma unroll 1
-    for (; ks + 1 < ksn; ks += 2) {
-      slice(ks, 0);
-      slice(ks + 1, 1);
+    for (; j + 1 < n8; j += 2) {
+      step8(j, 0);
+      step8(j + 1, 1);
     }
-    if (ks < ksn) slice(ks, 0);
+    if (j < n8) step8(j, 0);
+    if (ksn & 1) step4(ksn - 1, 1);
 #pragma unroll
     for (int ms = 0; ms < MS; ++ms)
 #pragma unroll
@@ -142,7 +169,8 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
         for (int q = 0; q < 4; ++q) D[ms][nt][q] = __dadd_rn(acc[0][ms][nt][q], acc[KS2 - 1][ms][nt][q]);
   } else {
 #pragma unroll 1
-    for (int ks = 0; ks < ksn; ++ks) slice(ks, 0);
+    for (int j = 0; j < n8; ++j) step8(j, 0);
+    if (ksn & 1) step4(ksn - 1, 0);
 #pragma unroll
     for (int ms = 0; ms < MS; ++ms)
 #pragma unroll

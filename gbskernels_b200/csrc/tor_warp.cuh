@@ -60,7 +60,7 @@ constexpr int kTorTD = 2 * kTorTail;               // tail rows (10)
 constexpr int kTorZE = kTorTD * (kTorTD + 1) / 2;  // packed lower tail entries (55)
 
 struct TorWLayout {
-  int col_off, inv_off, zd_off, det_off, gidx_off, rho_off, total;  // in doubles
+  int col_off, inv_off, zd_off, det_off, gidx_off, id_off, rho_off, total;  // in doubles
 };
 
 // rows = 2q prefix rows; column u holds rows - u prefix slots + 10 tail slots.
@@ -75,7 +75,8 @@ __host__ __device__ inline TorWLayout tor_w_layout(int kmax, bool cert) {
   Lw.zd_off = Lw.inv_off + rows + 1;
   Lw.det_off = Lw.zd_off + (q + 1) * kTorZE;
   Lw.gidx_off = Lw.det_off + q + 2;
-  Lw.rho_off = Lw.gidx_off + (rows + 2) / 2;
+  Lw.id_off = Lw.gidx_off + (rows + 2) / 2;  // packed 10 x 10 identity (excluded tail rows)
+  Lw.rho_off = Lw.id_off + kTorZE + 1;
   int total = Lw.rho_off + (cert ? 2 * kmax + 2 : 0);
   if (cert) {  // the sigma proof factors a packed 2k x 2k matrix (+ 2k scalings) in the col / zd region
     const int need = (2 * kmax) * (2 * kmax + 1) / 2 + 2 * kmax + 8;
@@ -83,6 +84,7 @@ __host__ __device__ inline TorWLayout tor_w_layout(int kmax, bool cert) {
       const int shift = need - Lw.det_off;
       Lw.det_off += shift;
       Lw.gidx_off += shift;
+      Lw.id_off += shift;
       Lw.rho_off += shift;
       total += shift;
     }
@@ -111,78 +113,77 @@ __device__ __forceinline__ void tor_tri_ij(int e, int& i, int& jj) {
 // Writes the two factor rows into columns 0..R0 (and L[R1][R0]), the two W rows
 // into the tail slots of columns R0 and R1, inv[R0], inv[R1], detat[c + 1] and
 // Zd[c + 1].  Returns false when a pivot is not positive (the walk continues with a
-// unit pivot; the instance is flagged).
+// unit pivot; the instance is flagged).  (zi, zj): this lane's Zd entries.
 __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int k, int q, int r, int j, int c,
                                              double* col, double* inv, double* zd, double* detat, int* gidx,
-                                             int lane) {
+                                             int lane, const int (&zi)[2], const int (&zj)[2]) {
   const int dim = 2 * k;
   const int rows = 2 * q;
   const int R0 = 2 * c, R1 = R0 + 1;
   const int gR0 = j, gR1 = j + k;
-  const int nx = R0 + 2 + 2 * r;
+  const int nx = R0 + 2 * r;
   if (lane == 0) {
     gidx[R0] = gR0;
     gidx[R1] = gR1;
   }
-  // residual slots x = lane, lane + 32: kind 1 = prefix column x (read L[x][v] at
-  // column offset x - v while x > v), 2 / 3 = the new diagonal slots, 4 = tail column
-  // (read W[v][jt] at offset rows + jt - v), 0 = idle
+  // residual slots x = lane, lane + 32: x < R0 = prefix column x (reads L[x][v], at
+  // column offset x - v, while v < x), R0 <= x < R0 + 2r = tail column x - R0
+  // (reads W[v][x - R0] at offset rows + x - R0 - v), beyond = idle
   double a[2], b[2];
-  int kind[2], off[2];
+  int lim[2], off[2];  // a slot reads column v at offset off - v while v < lim
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int x = lane + 32 * h;
     a[h] = 0.0;
     b[h] = 0.0;
-    kind[h] = x < R0 ? 1 : x == R0 ? 2 : x == R1 ? 3 : x < nx ? 4 : 0;
-    off[h] = kind[h] == 1 ? x : rows + (x - R0 - 2);
+    lim[h] = x < R0 ? x : (x < nx ? R0 : 0);
+    off[h] = x < R0 ? x : rows + (x - R0);
     if (x < R0) {
       const int gc = gidx[x];
       a[h] = tor_m(Oc, dim, gR0, gc);
       b[h] = tor_m(Oc, dim, gR1, gc);
-    } else if (x == R0) {
-      a[h] = tor_m(Oc, dim, gR0, gR0);
-      b[h] = tor_m(Oc, dim, gR1, gR0);
-    } else if (x == R1) {
-      b[h] = tor_m(Oc, dim, gR1, gR1);
     } else if (x < nx) {
-      const int gT = tor_tail_g(x - R0 - 2, q, k);
+      const int gT = tor_tail_g(x - R0, q, k);
       a[h] = tor_m(Oc, dim, gR0, gT);
       b[h] = tor_m(Oc, dim, gR1, gT);
     }
   }
-  // forward substitution over the existing columns v < R0
-  for (int v = 0; v < R0; ++v) {
-    const int owner = v & 31;
-    double* cv = col + tor_col_base(v, rows);
-    // the owner's finished residual, broadcast; every lane scales it (same value)
+  // the new 2 x 2 diagonal block, accumulated in every lane from the broadcast values
+  double d00 = tor_m(Oc, dim, gR0, gR0), d10 = tor_m(Oc, dim, gR1, gR0), d11 = tor_m(Oc, dim, gR1, gR1);
+  // forward substitution over the existing columns v < R0 (owners of v < 32 hold the
+  // residual in slot 0, the others in slot 1)
+  double* cv = col;  // column v starts at tor_col_base(v, rows)
+  auto step = [&](int v, double av, double bv) {
     const double iv = inv[v];
-    const double l0 = __shfl_sync(0xffffffffu, (v >> 5) ? a[1] : a[0], owner) * iv;
-    const double l1 = __shfl_sync(0xffffffffu, (v >> 5) ? b[1] : b[0], owner) * iv;
-    if (lane == owner) {
+    const double l0 = av * iv, l1 = bv * iv;
+    if (lane == (v & 31)) {
       cv[R0 - v] = l0;
       cv[R1 - v] = l1;
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int x = lane + 32 * h;
       double e = 0.0;  // 0 for finished or idle slots: fma(-0, l, a) == a
-      if ((kind[h] == 1 && x > v) || kind[h] == 4) e = cv[off[h] - v];
-      e = kind[h] == 2 ? l0 : (kind[h] == 3 ? l1 : e);
+      if (v < lim[h]) e = cv[off[h] - v];
       a[h] = fma(-e, l0, a[h]);
       b[h] = fma(-e, l1, b[h]);
     }
-  }
-  // the two diagonal slots
-  const int o0 = R0 & 31, h0 = R0 >> 5;
-  const int o1 = R1 & 31, h1 = R1 >> 5;
-  double s0 = __shfl_sync(0xffffffffu, h0 ? a[1] : a[0], o0);
-  const double m10 = __shfl_sync(0xffffffffu, h0 ? b[1] : b[0], o0);
+    d00 = fma(-l0, l0, d00);
+    d10 = fma(-l0, l1, d10);
+    d11 = fma(-l1, l1, d11);
+    cv += rows + kTorTD - v;
+  };
+  const int v1 = R0 < 32 ? R0 : 32;
+  for (int v = 0; v < v1; ++v)
+    step(v, __shfl_sync(0xffffffffu, a[0], v), __shfl_sync(0xffffffffu, b[0], v));
+  for (int v = 32; v < R0; ++v)
+    step(v, __shfl_sync(0xffffffffu, a[1], v & 31), __shfl_sync(0xffffffffu, b[1], v & 31));
+  // the two pivots (identical in every lane)
+  double s0 = d00;
   bool ok = s0 > 0.0;
   if (!ok) s0 = 1.0;
   const double i0 = rsqrt(s0);
-  const double l10 = m10 * i0;
-  double s1 = fma(-l10, l10, __shfl_sync(0xffffffffu, h1 ? b[1] : b[0], o1));
+  const double l10 = d10 * i0;
+  double s1 = fma(-l10, l10, d11);
   if (!(s1 > 0.0)) {
     ok = false;
     s1 = 1.0;
@@ -193,8 +194,8 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int x = lane + 32 * h;
-    if (x >= R0 + 2 && x < nx) {
-      const int jt = x - R0 - 2;
+    if (x >= R0 && x < nx) {
+      const int jt = x - R0;
       const double w0 = a[h] * i0;
       const double w1 = fma(-w0, l10, b[h]) * i1;
       c0[rows - R0 + jt] = w0;
@@ -217,12 +218,10 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
   for (int h = 0; h < 2; ++h) {
     const int e = lane + 32 * h;
     if (e < kTorZE) {
-      int i, jj;
-      tor_tri_ij(e, i, jj);
       double z = zs[e];
-      if (i < 2 * r) {
-        z = fma(-w0p[i], w0p[jj], z);
-        z = fma(-w1p[i], w1p[jj], z);
+      if (zi[h] < 2 * r) {
+        z = fma(-w0p[zi[h]], w0p[zj[h]], z);
+        z = fma(-w1p[zi[h]], w1p[zj[h]], z);
       }
       zt[e] = z;
     }
@@ -234,23 +233,27 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
 // One prefix leaf: every lane l < 2^r factors Z~ for the tail subset l.  Returns the
 // lane's signed term (0 for idle lanes); ok is cleared on a non-positive pivot and
 // the term dimension m = 2 (c + |T'|) is returned for the certified radius.
-__device__ __forceinline__ double tor_w_leaf(const double* zc, int r, int c, int k, double detc, int lane,
-                                             bool& ok, int& m) {
+// Rows of excluded tail modes are read from the packed identity zid, and their
+// pivot reciprocal is set to 0: every entry in an excluded row or column is then an
+// exact zero and every fused term it feeds is exact, so the included entries see
+// the same rounded operations as the factorisation of the compressed matrix.
+__device__ __forceinline__ double tor_w_leaf(const double* zc, const double* zid, int r, int c, int k, double detc,
+                                             int lane, bool& ok, int& m) {
   double term = 0.0;
   m = 0;
   if (lane < (1 << r)) {
     const int td = 2 * r;
     double Lz[kTorZE];  // off-diagonal entries (the diagonal slots stay unused)
-    double iv[kTorTD];  // 1 / L[i][i]
+    double iv[kTorTD];  // 1 / L[i][i] (0 for excluded rows)
     double det = 1.0;
 #pragma unroll
     for (int i = 0; i < kTorTD; ++i) {
       const bool in_i = i < td && ((lane >> (i >> 1)) & 1);
+      const double* zr = (in_i ? zc : zid) + i * (i + 1) / 2;
 #pragma unroll
       for (int jj = 0; jj <= i; ++jj) {
-        const bool in_j = jj < td && ((lane >> (jj >> 1)) & 1);
         const int e = i * (i + 1) / 2 + jj;
-        double s = (in_i && in_j) ? zc[e] : (i == jj ? 1.0 : 0.0);
+        double s = zr[jj];
 #pragma unroll
         for (int u = 0; u < jj; ++u) s = fma(-Lz[i * (i + 1) / 2 + u], Lz[jj * (jj + 1) / 2 + u], s);
         if (jj < i) {
@@ -260,7 +263,7 @@ __device__ __forceinline__ double tor_w_leaf(const double* zc, int r, int c, int
             ok = false;
             s = 1.0;
           }
-          iv[i] = in_i ? rsqrt(s) : 1.0;  // excluded rows: s == 1 exactly
+          iv[i] = in_i ? rsqrt(s) : 0.0;  // excluded rows: s == 1 exactly
           det *= s;
         }
       }
@@ -461,19 +464,24 @@ static __device__ bool tor_warp_item(const double* __restrict__ Oc, int k, int g
   double* zd = ws + Lw.zd_off;
   double* detat = ws + Lw.det_off;
   int* gidx = reinterpret_cast<int*>(ws + Lw.gidx_off);
-  // Zd[0] = M_TT (packed lower, tail rows < 2r; the rest unused)
+  double* zid = ws + Lw.id_off;
+  // Zd[0] = M_TT (packed lower, tail rows < 2r; the rest unused) and the identity
   for (int e = lane; e < kTorZE; e += 32) {
     int i, jj;
     tor_tri_ij(e, i, jj);
     zd[e] = (i < 2 * r) ? tor_m(Oc, dim, tor_tail_g(i, q, k), tor_tail_g(jj, q, k)) : 0.0;
+    zid[e] = i == jj ? 1.0 : 0.0;
   }
   if (lane == 0) detat[0] = 1.0;
+  int zi[2], zj[2];  // this lane's packed Zd entries (lane, lane + 32)
+#pragma unroll
+  for (int h = 0; h < 2; ++h) tor_tri_ij(lane + 32 * h < kTorZE ? lane + 32 * h : 0, zi[h], zj[h]);
   __syncwarp();
   bool ok = true;
   int count = 0;
   for (int j = 0; j < g; ++j)
     if ((pat >> j) & 1u) {
-      ok = tor_w_append(Oc, k, q, r, j, count, col, inv, zd, detat, gidx, lane) && ok;
+      ok = tor_w_append(Oc, k, q, r, j, count, col, inv, zd, detat, gidx, lane, zi, zj) && ok;
       ++count;
     }
   const int pc = count;
@@ -486,11 +494,11 @@ static __device__ bool tor_warp_item(const double* __restrict__ Oc, int k, int g
       const int z = __ffsll((long long)Tm) - 1;
       const int jz = g + rp - 1 - z;
       count = pc + __popcll((long long)(Tm >> (z + 1)));
-      ok = tor_w_append(Oc, k, q, r, jz, count, col, inv, zd, detat, gidx, lane) && ok;
+      ok = tor_w_append(Oc, k, q, r, jz, count, col, inv, zd, detat, gidx, lane, zi, zj) && ok;
       ++count;
     }
     int m = 0;
-    const double t = tor_w_leaf(zd + count * kTorZE, r, count, k, detat[count], lane, ok, m);
+    const double t = tor_w_leaf(zd + count * kTorZE, zid, r, count, k, detat[count], lane, ok, m);
     if (CERT) {
       // ball butterfly: the value operations are those of warp_sum_d
       double v = t;

@@ -155,6 +155,9 @@ const char* gbs_haf_noalloc_last_error(void);
  * FP64 tensor-core throughput of this GPU (mma .m16n8k8 .f64 chains on every SM),
  * the denominator of the kernels' roofline fraction.  No reference counterpart.  */
 int gbs_probe_fp64_peak(double* tflops, float* ms);
+/* the same probe for one mma shape: k = 8 (m16n8k8, = gbs_probe_fp64_peak) or
+ * k = 4 (m16n8k4); flops counted per shape.  No reference counterpart.           */
+int gbs_probe_fp64_mma(int k, double* tflops, float* ms);
 
 #ifdef __cplusplus
 }

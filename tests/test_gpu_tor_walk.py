@@ -81,3 +81,13 @@ def test_tor_certified_non_pd_is_refused(gpu):
     O_bad = (O_bad + O_bad.T) / 2
     with pytest.raises(FloatingPointError):
         gpu.tor_batched(O_bad[None], precision="certified", return_diagnostics=True)
+
+
+def test_workload_runner_small_torontonian(gpu):
+    from gbskernels_b200 import configs, workloads
+    mats = list(workloads.tor_click_batch(16, kmin=10, kmax=14, seed=9))
+    res, out, aux, st = configs.run("tor", mats, "certified")
+    assert res["status_ok"] == 16 and res["launches"] == 1 and res["kernel_ms"] > 0
+    with gpu.Workspace() as ws:
+        assert np.array_equal(out, ws.tor_batched(mats))
+    assert np.all(aux > 0)
