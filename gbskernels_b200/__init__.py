@@ -46,6 +46,7 @@ _GPU_MAX_DIM = {
     "lhaf": 32, "lhaf_dd": 32,
     "tor": 48, "tor_dd": 48,
 }
+_TOR_COMPLEX_MAX_DIM = 24  # complex O (subset LU path), the reference's GPU cap
 
 
 # ------------------------------------------------------------------ helpers
@@ -88,7 +89,14 @@ def _prepare(func: str, matrices: Iterable[Any], precision: str) -> np.ndarray:
         if precision == "dd":
             raise ValueError("GPU torontonian (precision='dd') is real-domain only; the input "
                              "has non-zero imaginary parts.")
+        if d > _TOR_COMPLEX_MAX_DIM:
+            raise ValueError(f"GPU torontonian of a complex O (subset LU): dimension {d} exceeds "
+                             f"the limit {_TOR_COMPLEX_MAX_DIM}")
     return stack
+
+
+def _is_complex_tor(func: str, stack: np.ndarray) -> bool:
+    return func == "tor" and stack.size > 0 and float(np.max(np.abs(stack.imag))) > 0.0
 
 
 def _kernel_dim(func: str, d: int) -> int:
@@ -133,7 +141,16 @@ def _auto_batched(func: str, matrices, return_diagnostics: bool):
     out = np.empty(B, dtype=np.complex128)
     kappa = np.empty(B, dtype=np.float64)
     tier = np.empty(B, dtype=np.int32)
-    if B:
+    if B and _is_complex_tor(func, stack):
+        # complex O: the indicator pass runs (subset LU), but the double-double rerun
+        # is real-domain only -- refuse like the reference's GPU dd torontonian
+        out, kappa = _call_aux(func, stack, "kappa")
+        kappa = kappa / np.maximum(np.abs(out), 1e-300)
+        if np.any(kappa >= _AUTO_KAPPA_MAX):
+            raise ValueError("precision='auto' would rerun a complex torontonian in double-double, "
+                             "which is real-domain only; use precision='fp64'")
+        tier[:] = 0
+    elif B:
         rc = lib.gbs_auto_host(_FN[func], _lib.dptr(stack.view(np.float64)), d, B, _AUTO_KAPPA_MAX,
                                _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier))
         _lib.check(rc, "gbs_auto_host")
@@ -171,6 +188,9 @@ def _certified_batched(func: str, matrices, rtol: float | None):
     an element that neither rung certifies to rtol raises FloatingPointError)."""
     stack = _prepare(func, matrices, "fp64")
     _check_certified_input(stack)
+    if _is_complex_tor(func, stack):
+        raise NotImplementedError("certified torontonian is real-domain only (the bound rests on the "
+                                  "Cholesky factor of I - O_S); the input has non-zero imaginary parts")
     values, bounds = _call_aux(func, stack, "certified")
     out = values.astype(np.complex128, copy=True)
     diags = []
@@ -308,7 +328,7 @@ def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: b
     A = np.asarray(O)
     if np.iscomplexobj(A):
         if np.any(np.imag(A) != 0):
-            raise ValueError("tor_single is real-domain only; use tor() for complex O (dim <= 48)")
+            raise ValueError("tor_single is real-domain only; use tor() for complex O (dim <= 24)")
         A = np.real(A)
     M = np.ascontiguousarray(A, dtype=np.float64)
     if M.ndim != 2 or M.shape[0] != M.shape[1] or M.shape[0] % 2 != 0:

@@ -15,6 +15,7 @@
 #include "haf_pt.cuh"
 #include "perm_tor.cuh"
 #include "cert.cuh"
+#include "tor_lu.cuh"
 #include "tor_warp.cuh"
 
 namespace gbsb {
@@ -159,7 +160,28 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
   const int n = d.dim / 2;
   const int dim = d.dim;
   const double* Oc = mats + d.off;
-  if (TIER != kTierDD) {
+  if (!d.real_in) {
+    // complex O (binary64 tiers only; the host refuses the others): one warp per
+    // subset LU, w.count masks from w.lo (tor_lu.cuh)
+    if constexpr (TIER == kTierFp64 || TIER == kTierKappa) {
+      cplx acc = mkc(0.0, 0.0);
+      double aabs = 0.0;
+      bool sing = false;
+      for (unsigned long long k = 0; k < w.count; ++k) {
+        const cplx t = tor_lu_term(Oc, n, (uint32_t)(w.lo + k), ws, lane, sing);
+        acc = cadd(acc, t);
+        if (TIER == kTierKappa) aabs += hypot(t.re, t.im);
+        __syncwarp();
+      }
+      r.val = ddc_from_c(acc);
+      r.aux = aabs;
+      if (sing) r.st = kStOffDomain;
+    } else {
+      r.st = kStTooLarge;
+    }
+    return r;
+  }
+  if constexpr (TIER != kTierDD) {
     // binary64 tiers: warp-cooperative prefix walk with the 32-subset register tail
     // (tor_warp.cuh); one work item = w.count prefix patterns over the first d.param
     // prefix modes, walked one after another by the whole warp
@@ -196,7 +218,7 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
     if (!proved || !ok) r.st = TIER == kTierCert ? kStUncertified : kStOffDomain;
     __syncwarp();
     return r;
-  }
+  } else {
   // double-double tier: one lane per prefix pattern, each walking its own subtree
   // (perm_tor.cuh); the real part of O is staged in the warp's shared workspace
   for (int e = lane; e < dim * dim; e += 32) ws[e] = Oc[2 * e];
@@ -215,6 +237,7 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
   if (!__all_sync(0xffffffffu, ok)) r.st = kStOffDomain;
   __syncwarp();
   return r;
+  }
 }
 
 // ------------------------------------------------------------------ the item kernel

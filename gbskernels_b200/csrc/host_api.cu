@@ -28,6 +28,7 @@
 #include "gbs_kernels.cuh"
 #include "haf_dd.cuh"
 #include "haf_pt.cuh"
+#include "tor_lu.cuh"
 #include "tor_warp.cuh"
 
 namespace gbsb {
@@ -140,6 +141,10 @@ static double item_cost(int fn, int dim, unsigned long long count, int tier, int
       // binary64 tiers: count prefix patterns, 2^(q - g) leaves of 32 subsets each
       // (g = param); double-double: count lanes of 2^(n - g) subsets each
       const int n = dim / 2, q = n - std::min(n, 5);
+      if (param < 0) {  // complex O: count subset LU factorisations
+        c = (double)count * dim * dim * dim;
+        break;
+      }
       c = tier == kTierDD ? (double)count * std::ldexp(1.0, n - param) * n * n
                           : (double)count * std::ldexp(1.0, q - param) * 32.0 * (36.0 * q + 1400.0);
       break;
@@ -186,6 +191,11 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     const unsigned long long cnt = 1ull << per;
     for (unsigned long long lo = 0; lo < masks; lo += cnt) add(lo, std::min(cnt, masks - lo));
     P.haf_smax = std::max(P.haf_smax, dim_eval);
+  } else if (!real_in) {  // tor, complex O: ranges of subset masks, one LU per subset
+    const int n = dim_eval / 2;
+    const int per = std::min(n, 6);
+    for (unsigned long long lo = 0; lo < (1ull << n); lo += (1ull << per)) add(lo, 1ull << per);
+    d.param = -1;
   } else if (tier == kTierDD) {  // tor, double-double: one lane per prefix pattern
     const int n = dim_eval / 2;
     const int g = std::max(std::min(n, 5), n - 7);
@@ -214,6 +224,7 @@ static int ws_for_plan(const Plan& P) {
     const int fn = d.ft >> 2, tier = d.ft & 3;
     int w = 0;
     if (fn == kFnPerm) w = 2 * d.dim * d.dim;
+    else if (fn == kFnTor && !d.real_in) w = tor_lu_ws_doubles();
     else if (fn == kFnTor) w = tier == kTierDD ? d.dim * d.dim : tor_w_layout(d.dim / 2, tier == kTierCert).total;
     else if (tier == kTierDD) w = haf_dd_layout(P.haf_smax).total;
     else w = haf_layout(P.haf_smax, tier == kTierCert).total;
@@ -344,7 +355,18 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
         for (size_t i = 0; i < nn; ++i)
           if (r.mat[2 * i + 1] != 0.0) { re = false; break; }
       }
-      if (!re) return fail(cudaErrorNotSupported, "torontonian: complex O is not supported by the batched kernel");
+      if (!re) {
+        // complex O: subset LU determinants, binary64 tiers, the reference's GPU cap
+        if (r.tier == kTierDD || r.tier == kTierCert || r.single)
+          return fail(cudaErrorNotSupported,
+                      "torontonian: complex O is supported in the fp64 tier only (the double-double, "
+                      "certified and single-large paths are real-domain)");
+        if (r.dim / 2 > kTorLuMaxModes)
+          return fail(cudaErrorInvalidValue, "torontonian: complex O above the cap of 12 modes");
+        *real_in = false;
+        *dim_eval = r.dim;
+        return 0;
+      }
       *real_in = true;
       *dim_eval = r.dim;
       return 0;

@@ -45,8 +45,8 @@ def _batched(G, func):
 @pytest.mark.parametrize("precision", ["fp64", "dd"])
 def test_golden_vectors(gpu, golden, func, precision):
     for m, truth, _, i in golden_cases(golden, func):
-        if func == "tor" and np.any(np.imag(m) != 0):
-            continue  # complex O: not a batched-kernel input (the API rejects it)
+        if func == "tor" and np.any(np.imag(m) != 0) and precision == "dd":
+            continue  # complex O: the double-double torontonian is real-domain only
         v = _batched(gpu, func)(m[None], precision=precision)[0]
         tol = FP64_TOL if precision == "fp64" else DD_TOL
         if abs(truth) < 1e-6:
@@ -58,8 +58,6 @@ def test_golden_vectors(gpu, golden, func, precision):
 @pytest.mark.parametrize("func", ["perm", "haf", "lhaf", "tor"])
 def test_golden_indicator(gpu, golden, func):
     for m, truth, _, i in golden_cases(golden, func):
-        if func == "tor" and np.any(np.imag(m) != 0):
-            continue
         if abs(truth) < 1e-6:
             continue  # kappa is ill-defined at a zero value
         v, diags = _batched(gpu, func)(m[None], precision="auto", return_diagnostics=True)
@@ -279,3 +277,41 @@ def test_workspace_resident_output(gpu):
         assert np.array_equal(host, gpu.haf_batched(mats))
         assert np.array_equal(t.cpu().numpy(), host)
         res.close()
+
+
+# ---------------------------------------------------------------- complex torontonian (subset LU)
+def complex_O(n, scale=0.3):
+    X = RNG.standard_normal((2 * n, 2 * n)) + 1j * RNG.standard_normal((2 * n, 2 * n))
+    return scale * (X + X.T) / (2 * np.sqrt(2 * n))
+
+
+@pytest.mark.parametrize("n", [1, 3, 6, 9, 12])
+def test_tor_complex_vs_binary128_oracle(gpu, orc, n):
+    mats = np.stack([complex_O(n) for _ in range(2)])
+    got = gpu.tor_batched(mats)
+    for i in range(2):
+        truth, absn = orc.tor(mats[i], "quad", with_absnorm=True)
+        kappa = absn / abs(truth)  # sum |term| / |tor|
+        assert rel_err(got[i], truth) < max(FP64_TOL, 1e-15 * kappa), (n, i, kappa)
+        if kappa < 1e8:  # the auto tier keeps the binary64 value (no double-double rerun)
+            v, d = gpu.tor_batched(mats[i:i + 1], precision="auto", return_diagnostics=True)
+            assert v[0] == got[i] and d[0]["tier"] == "fp64"
+            assert d[0]["cancellation"] == pytest.approx(kappa, rel=1e-6)
+        else:
+            with pytest.raises(ValueError, match="real-domain"):
+                gpu.tor_batched(mats[i:i + 1], precision="auto")
+
+
+def test_tor_complex_contract(gpu):
+    O = complex_O(4)[None]
+    with pytest.raises(ValueError, match="real-domain"):
+        gpu.tor_batched(O, precision="dd")
+    with pytest.raises(NotImplementedError, match="real-domain"):
+        gpu.tor_batched(O, precision="certified", return_diagnostics=True)
+    with pytest.raises(ValueError, match="limit 24"):
+        gpu.tor_batched(complex_O(13)[None])
+    with gpu.Workspace() as ws:  # ragged mix of real and complex O in one queue
+        mats = [complex_O(3), np.real(complex_O(5)), complex_O(2)]
+        together = ws.tor_batched(mats)
+    alone = np.array([gpu.tor_batched(m[None])[0] for m in mats])
+    assert np.array_equal(together, alone)
