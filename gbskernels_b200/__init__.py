@@ -30,7 +30,7 @@ from . import _lib
 __version__ = "0.1.0"
 __all__ = [
     "perm", "perm_batched", "haf", "haf_batched", "lhaf", "lhaf_batched",
-    "tor", "tor_batched", "tor_single", "gpu_available", "gpu_backend_kind",
+    "tor", "tor_batched", "tor_single", "lhaf_repeated", "gpu_available", "gpu_backend_kind",
     "Workspace", "PRECISIONS", "queue_evaluate", "Server", "serve_stream",
 ]
 
@@ -314,6 +314,53 @@ def tor_batched(matrices: Iterable[Any], precision: str = "fp64", backend: str =
                 return_diagnostics: bool = False, rtol: float | None = None):
     """Torontonians of a (B, 2n, 2n) batch -> complex128 vector."""
     return _dispatch_batched("tor", matrices, precision, backend, return_diagnostics, rtol)
+
+
+def lhaf_repeated(A: Any, gamma: Any, reps: Any, backend: str = "gpu", certified: bool = False):
+    """Loop hafnians of ``A`` expanded by repetition patterns
+    (gbskernels/__init__.py:561-632 contract).
+
+    ``A`` is the (M, M) base matrix, ``gamma`` the length-M loop weights (``None`` ->
+    zeros: the ordinary hafnian of the expansion), ``reps`` a (B, M) table of
+    non-negative counts (or one length-M pattern).  Returns the (B,) values (a scalar
+    for one pattern) of the finite-difference sieve, ``prod(n_i + 1)`` terms per
+    pattern, evaluated on the GPU (``libgbs_b200`` sieve kernel).  Caps: M <= 32,
+    sum(reps) <= 64, prod(n_i + 1) <= 2^40.  ``certified=True`` (the reference's
+    certified sieve) is not provided and raises RuntimeError."""
+    _check_backend(backend)
+    A = np.ascontiguousarray(A, dtype=np.complex128)
+    if A.ndim != 2 or A.shape[0] != A.shape[1]:
+        raise ValueError(f"lhaf_repeated: A must be square (M, M), got {A.shape}")
+    M = A.shape[0]
+    g = (np.zeros(M, dtype=np.complex128) if gamma is None
+         else np.ascontiguousarray(gamma, dtype=np.complex128))
+    if g.shape != (M,):
+        raise ValueError(f"lhaf_repeated: gamma must be a length-{M} vector, got {g.shape}")
+    r = np.ascontiguousarray(reps, dtype=np.int32)
+    single = r.ndim == 1
+    if single:
+        r = r[None, :]
+    if r.ndim != 2 or r.shape[1] != M:
+        raise ValueError(f"lhaf_repeated: reps must be (B, {M}) or ({M},), got {np.asarray(reps).shape}")
+    if (r < 0).any():
+        raise ValueError("lhaf_repeated: reps must be non-negative")
+    if certified:
+        raise RuntimeError("lhaf_repeated(certified=True) is not in this build")
+    if M > 32:
+        raise ValueError(f"lhaf_repeated: M = {M} exceeds the cap 32")
+    if r.size and int(r.sum(axis=1).max()) > 64:
+        raise ValueError("lhaf_repeated: sum(reps) exceeds the cap 64")
+    B = r.shape[0]
+    out = np.empty(B, dtype=np.complex128)
+    if B:
+        lib = _lib.load()
+        rc = lib.gbs_lhaf_repeated_host(_lib.dptr(A.view(np.float64)), _lib.dptr(g.view(np.float64)), M,
+                                        _lib.iptr(r), B, _lib.dptr(out.view(np.float64)))
+        if rc != 0:
+            msg = lib.gbs_lhaf_repeated_last_error()
+            raise (ValueError if rc == 1 else RuntimeError)(
+                f"lhaf_repeated failed (code {rc}): {msg.decode() if msg else ''}")
+    return complex(out[0]) if single else out
 
 
 def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: bool = False):

@@ -56,6 +56,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_queue_prepare": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int], ctypes.c_int),
     "gbs_queue_run": ([_vp, _vp], ctypes.c_int),
     "gbs_queue_read": ([_vp, _vp, _dp, _dp, _ip], ctypes.c_int),
+    "gbs_lhaf_repeated_host": ([_dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _dp], ctypes.c_int),
+    "gbs_lhaf_repeated_last_error": ([], ctypes.c_char_p),
     "gbs_probe_fp64_peak": ([_dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "gbs_probe_fp64_mma": ([ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "gbs_haf_noalloc": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp], ctypes.c_int),

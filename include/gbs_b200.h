@@ -71,6 +71,17 @@ int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, do
 int gbs_tor_recursive_single_host(const double* O, int n, int g, double* out);
 int gbs_tor_single_certified_host(const double* O, int n, int g, double* out, double* bound);
 
+/* ---- repeated-row loop hafnian (finite-difference sieve) ----------------------
+ * reference: core/host_api.cu:409-432 (gbs_lhaf_repeated_host),
+ * bindings/gbskernels_ext.cpp:49; algorithm cpu_ref/repeated.py:64-122.
+ * A: M x M complex base matrix; gamma: M complex loop weights (NULL = zeros, the
+ * ordinary hafnian of the expansion); reps: batch x M non-negative counts; out:
+ * batch complex values lhaf(A repeated by reps[b]).  Caps: M <= 32, N = sum(reps[b])
+ * <= 64, prod(reps[b][i] + 1) <= 2^40.  The reference's certified variant
+ * (gbs_lhaf_repeated_cert_host) is not provided.                                */
+int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out);
+const char* gbs_lhaf_repeated_last_error(void);
+
 /* ---- auto tier on the device ----------------------------------------------
  * reference: gbskernels/__init__.py:272-297 (_gpu_auto_batched) whose fp64 pass is
  * gbs_*_kappa_host and whose rerun is gbs_*_dd_host; here both run in the library.

@@ -123,6 +123,26 @@ def tor(O, prec: str = "fp64", hilo: bool = False, with_absnorm: bool = False):
     return (v, absn) if with_absnorm else v
 
 
+def lhaf_repeated(A, gamma, reps, prec: str = "fp64"):
+    """Loop hafnian of A with row/col i repeated reps[i] times (loop weight gamma[i]
+    on every copy), by the finite-difference sieve (cpu_ref/repeated.py:64-122)."""
+    lib = _load_oracle()
+    A = np.ascontiguousarray(A, dtype=np.complex128)
+    M = A.shape[0]
+    g = np.zeros(M, np.complex128) if gamma is None else np.ascontiguousarray(gamma, dtype=np.complex128)
+    r = np.ascontiguousarray(reps, dtype=np.int32)
+    out = np.zeros(4)
+    fn = lib.orc_lhaf_repeated
+    fn.argtypes = [_dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp]
+    fn.restype = ctypes.c_int
+    rc = fn(A.view(np.float64).ctypes.data_as(_dp), g.view(np.float64).ctypes.data_as(_dp),
+            r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), M, 0 if prec == "fp64" else 1,
+            out.ctypes.data_as(_dp))
+    if rc:
+        raise ValueError("orc_lhaf_repeated: bad arguments")
+    return _value(out, False)
+
+
 def tor_complex(O, prec: str = "fp64"):
     O = np.asarray(O)
     out, _ = _call("orc_tor_complex", O, O.shape[0] // 2, 0 if prec == "fp64" else 1)

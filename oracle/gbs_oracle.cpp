@@ -13,6 +13,8 @@
 //   * torontonian, recursive prefix Cholesky (real)  core/tor_recursive.cu:41-115,
 //                                                   cpu_ref/tor_recursive.py:46-100
 //   * torontonian, per-subset determinant (complex)  cpu_ref/torontonian.py:48-64
+//   * loop hafnian of a repeated-row expansion,
+//     finite-difference sieve ....................... cpu_ref/repeated.py:64-122
 //   * sum|term| indicators for precision="auto" ..... cpu_ref/diagnostics.py:40-170,
 //                                                   core/permanent.cu:94-130
 //
@@ -24,6 +26,7 @@
 
 #include <quadmath.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -334,6 +337,77 @@ template <class T> void tor_real(const double* O, int n, double* out, double* ab
   if (absnorm) *absnorm = tr.abs_acc;
 }
 
+// Loop hafnian of A (M x M) with row / column i repeated reps[i] times and loop
+// weight gamma[i] on every copy: the finite-difference sieve of
+// cpu_ref/repeated.py:64-122 (same enumeration order: all v <= reps in row-major
+// odometer order, the v <-> reps - v symmetry keeping v lexicographically <= its
+// mirror and doubling the strict half; S_N by the mu-power ladder and the running
+// sigma^2 power, as there).
+template <class T> Cx<T> lhaf_sieve(const double* A, const double* g, const int* reps, int M) {
+  int N = 0;
+  for (int i = 0; i < M; ++i) N += reps[i];
+  if (N == 0) return {T(1), T(0)};
+  const int kmax = N / 2;
+  std::vector<T> coeff(kmax + 1);
+  for (int k = 0; k <= kmax; ++k) {
+    // C(N, 2k) (2k-1)!! accumulated in T
+    T c = T(1);
+    for (int t = 1; t <= 2 * k; ++t) c = c * T(N - 2 * k + t) / T(t);
+    for (int t = 2 * k - 1; t > 0; t -= 2) c = c * T(t);
+    coeff[k] = c;
+  }
+  auto binom = [](int n, int k) {
+    T c = T(1);
+    for (int t = 1; t <= k; ++t) c = c * T(n - k + t) / T(t);
+    return c;
+  };
+  std::vector<int> v(M, 0);
+  std::vector<T> x(M);
+  Cx<T> total{T(0), T(0)};
+  for (;;) {
+    // lexicographic comparison of v with its mirror reps - v
+    int cmp = 0;
+    for (int i = 0; i < M && cmp == 0; ++i) {
+      const int mi = reps[i] - v[i];
+      cmp = v[i] < mi ? -1 : (v[i] > mi ? 1 : 0);
+    }
+    if (cmp <= 0) {
+      int vs = 0;
+      for (int i = 0; i < M; ++i) vs += v[i];
+      T c = (vs % 2 == 0) ? T(1) : T(-1);
+      if (cmp < 0) c = c * T(2);
+      for (int i = 0; i < M; ++i) c = c * binom(reps[i], v[i]);
+      for (int i = 0; i < M; ++i) x[i] = T(reps[i] - 2 * v[i]);
+      Cx<T> sig2{T(0), T(0)}, mu{T(0), T(0)};
+      for (int i = 0; i < M; ++i) {
+        Cx<T> row{T(0), T(0)};
+        for (int j = 0; j < M; ++j)
+          row = cadd(row, cscale(Cx<T>{T(A[2 * (i * M + j)]), T(A[2 * (i * M + j) + 1])}, x[j]));
+        sig2 = cadd(sig2, cscale(row, x[i]));
+        mu = cadd(mu, cscale(Cx<T>{T(g[2 * i]), T(g[2 * i + 1])}, x[i]));
+      }
+      std::vector<Cx<T>> mupow(kmax + 1);
+      mupow[kmax] = (N % 2) ? mu : Cx<T>{T(1), T(0)};
+      const Cx<T> mu2 = cmul(mu, mu);
+      for (int k = kmax - 1; k >= 0; --k) mupow[k] = cmul(mupow[k + 1], mu2);
+      Cx<T> SN{T(0), T(0)}, sk{T(1), T(0)};
+      for (int k = 0; k <= kmax; ++k) {
+        SN = cadd(SN, cmul(cscale(sk, coeff[k]), mupow[k]));
+        sk = cmul(sk, sig2);
+      }
+      total = cadd(total, cscale(SN, c));
+    }
+    int i = M - 1;  // odometer, last index fastest (numpy ndindex order)
+    while (i >= 0 && v[i] == reps[i]) v[i--] = 0;
+    if (i < 0) break;
+    ++v[i];
+  }
+  T D = T(1);
+  for (int t = 2; t <= N; ++t) D = D * T(t);
+  for (int t = 0; t < N; ++t) D = D * T(2);
+  return cscale(total, T(1) / D);
+}
+
 }  // namespace
 
 extern "C" {
@@ -375,6 +449,22 @@ int orc_tor_complex(const double* O, int n, int prec, double* out, double* absno
   if (n == 0) { out[0] = 1.0; out[1] = out[2] = out[3] = 0.0; if (absnorm) *absnorm = 1.0; return 0; }
   if (prec == 0) put_c(tor_subset_det<double>(load<double>(O, 2 * n), n, absnorm), out);
   else put_c(tor_subset_det<__float128>(load<__float128>(O, 2 * n), n, absnorm), out);
+  return 0;
+}
+
+// Repeated-row loop hafnian (finite-difference sieve): A (M x M complex), gamma (M
+// complex, may be null = 0), reps (M ints).
+int orc_lhaf_repeated(const double* A, const double* gamma, const int* reps, int M, int prec, double* out) {
+  if (M < 0 || M > 64) return 1;
+  std::vector<double> g0;
+  if (!gamma) {
+    g0.assign(2 * (size_t)std::max(M, 1), 0.0);
+    gamma = g0.data();
+  }
+  for (int i = 0; i < M; ++i)
+    if (reps[i] < 0) return 1;
+  if (prec == 0) put_c(lhaf_sieve<double>(A, gamma, reps, M), out);
+  else put_c(lhaf_sieve<__float128>(A, gamma, reps, M), out);
   return 0;
 }
 
