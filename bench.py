@@ -59,6 +59,8 @@ def _args():
     ap.add_argument("--no-per-size", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--tuned", default=None,
+                    help="apply an autotuner table (gbskernels_b200.autotune JSON) before timing")
     ap.add_argument("--profile-small", action="store_true",
                     help="small case for ncu captures: 256 instances, 1 step, no extras")
     return ap.parse_args()
@@ -241,6 +243,9 @@ def main():
     from gbskernels_b200 import _lib, workloads
     lib = _lib.load()
 
+    if a.tuned:
+        from gbskernels_b200 import autotune
+        autotune.load(a.tuned)
     B = 256 if a.profile_small else a.batch
     funcs, mats = workloads.mixed_haf_lhaf(B, seed=a.seed + dist.rank)
     fcode = np.array([{"haf": 1, "lhaf": 2}[f] for f in funcs], dtype=np.int32)

@@ -55,6 +55,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_session_last_stats": ([_vp, _dp, _ip, _llp], ctypes.c_int),
     "gbs_queue_prepare": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int], ctypes.c_int),
     "gbs_queue_run": ([_vp, _vp], ctypes.c_int),
+    "gbs_session_set_graphs": ([_vp, ctypes.c_int], ctypes.c_int),
+    "gbs_set_split": ([ctypes.c_int] * 5, ctypes.c_int),
+    "gbs_get_split": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip], ctypes.c_int),
     "gbs_queue_read": ([_vp, _vp, _dp, _dp, _ip], ctypes.c_int),
     "gbs_lhaf_repeated_host": ([_dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _dp], ctypes.c_int),
     "gbs_lhaf_repeated_last_error": ([], ctypes.c_char_p),

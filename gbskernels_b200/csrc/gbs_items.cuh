@@ -9,6 +9,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "gbs_common.cuh"
 #include "gbs_kernels.cuh"
 #include "haf_dd.cuh"
@@ -17,11 +20,10 @@
 #include "cert.cuh"
 #include "tor_lu.cuh"
 #include "tor_warp.cuh"
+#include "tor_warp_dd.cuh"
 
 namespace gbsb {
 
-constexpr int kTorBatchMaxModes = 24;  // batched torontonian cap (dim 48)
-constexpr int kTorPackedMax = (2 * kTorBatchMaxModes) * (2 * kTorBatchMaxModes + 1) / 2;
 
 // ------------------------------------------------------------------ item evaluators
 struct ItemResult {
@@ -219,24 +221,20 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
     __syncwarp();
     return r;
   } else {
-  // double-double tier: one lane per prefix pattern, each walking its own subtree
-  // (perm_tor.cuh); the real part of O is staged in the warp's shared workspace
-  for (int e = lane; e < dim * dim; e += 32) ws[e] = Oc[2 * e];
-  __syncwarp();
-  const bool active = (unsigned long long)lane < w.count;
-  const uint32_t pat = (uint32_t)(w.lo + lane);
-  bool ok = true;
-  double absacc = 0.0;
-  dd total = dd_make(0.0);
-  if (active) {
-    dd L[kTorPackedMax];
-    ok = tor_lane_subtree<dd>(ws, n, d.param, pat, L, total, absacc, false);
-  }
-  const dd v = ok ? total : dd_make(0.0);
-  r.val = warp_sum_ddc(ddc{v, dd_make(0.0)});
-  if (!__all_sync(0xffffffffu, ok)) r.st = kStOffDomain;
-  __syncwarp();
-  return r;
+    // double-double tier: the same walk in double-word arithmetic with a 16-subset
+    // tail (tor_warp_dd.cuh); one work item = w.count prefix patterns
+    const TorDLayout Lw = tor_d_layout(n);
+    dd val = dd_make(0.0);
+    bool ok = true;
+    for (unsigned long long p = 0; p < w.count; ++p) {
+      dd t = dd_make(0.0);
+      ok = tor_dd_item(Oc, n, d.param, (uint32_t)(w.lo + p), ws, Lw, lane, t) && ok;
+      val = p == 0 ? t : dd_add(val, t);
+    }
+    r.val = ddc{val, dd_make(0.0)};
+    if (!ok) r.st = kStOffDomain;
+    __syncwarp();
+    return r;
   }
 }
 
@@ -350,10 +348,28 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
 
 // ------------------------------------------------------------------ launch helpers
 template <unsigned BR>
+static cudaError_t ensure_smem_br(size_t smem) {
+  // the kernel's dynamic shared-memory limit only grows; once it is high enough no
+  // attribute call is made, so a launch inside a stream capture issues none
+  // (per device: the attribute belongs to the device's context)
+  constexpr int kDevs = 64;
+  static std::atomic<size_t> smem_set[kDevs];
+  static std::mutex mu;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) dev = 0;
+  if (smem <= smem_set[dev].load()) return cudaSuccess;
+  std::lock_guard<std::mutex> lk(mu);
+  if (smem <= smem_set[dev].load()) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(gbs_items_kernel<BR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) smem_set[dev].store(smem);
+  return e;
+}
+
+template <unsigned BR>
 static cudaError_t launch_br(const ItemLaunch& P, int grid, int warps, cudaStream_t stream) {
   const size_t smem = (size_t)warps * P.ws_doubles * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(gbs_items_kernel<BR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  const cudaError_t e = ensure_smem_br<BR>(smem);
   if (e != cudaSuccess) return e;
   gbs_items_kernel<BR><<<grid, warps * 32, smem, stream>>>(P);
   return cudaGetLastError();
@@ -362,9 +378,7 @@ static cudaError_t launch_br(const ItemLaunch& P, int grid, int warps, cudaStrea
 template <unsigned BR>
 static int occ_br(const ItemLaunch& P, int warps) {
   const size_t smem = (size_t)warps * P.ws_doubles * sizeof(double);
-  if (cudaFuncSetAttribute(gbs_items_kernel<BR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-      cudaSuccess)
-    return 0;
+  if (ensure_smem_br<BR>(smem) != cudaSuccess) return 0;
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, gbs_items_kernel<BR>, warps * 32, smem) != cudaSuccess)
     return 0;

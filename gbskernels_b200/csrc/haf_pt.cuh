@@ -49,7 +49,7 @@ __host__ __device__ inline int haf_strips(int s) { return (s + 15) / 16; }
 // Batched Newton recurrence: the traces of kHafRing consecutive subsets are parked
 // in a ring (slot: kg[1..n] and the sign), then kHafRing lanes run one recurrence
 // each.  Slot k[0] holds (sign, 0) or (0, 0) for an empty subset.
-constexpr int kHafRing = 16;
+constexpr int kHafRing = 8;
 constexpr int kHafRingSlot = kHafMaxPairs + 1;  // complex entries per slot
 
 struct HafLayout {
@@ -440,8 +440,13 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   __syncwarp();
   const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
   // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
-  for (int e = lane; e < rows * ccols; e += 32) {
-    const int r = e / ccols, c = e - r * ccols;
+  const int dr = 32 / ccols, dc = 32 - dr * ccols;  // (r, c) advance per 32 elements
+  int r = lane / ccols, c = lane - (lane / ccols) * ccols;
+  for (int e = lane; e < rows * ccols; e += 32, r += dr, c += dc) {
+    if (c >= ccols) {
+      c -= ccols;
+      ++r;
+    }
     cplx v = mkc(0.0, 0.0);
     if (c < s && r < s) {
       const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
@@ -484,13 +489,17 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   __syncwarp();
 
   if (loop) {
-    // v_k = 1/2 sum_i y_a[i^1] y_b[i],  a = (k-1)/2, b = k-1-a
-    for (int k = 1; k <= n; ++k) {
+    // v_k = 1/2 sum_i y_a[i^1] y_b[i],  a = (k-1)/2, b = k-1-a: lane k-1 sums over i
+    // (sequentially, in i order) -- one pass for all k instead of a butterfly per k
+    if (lane < n) {
+      const int k = lane + 1;
       const int aa = (k - 1) >> 1, bb = k - 1 - aa;
       cplx t = mkc(0.0, 0.0);
-      if (lane < s) t = cmul(ld_c(Y + ((lane ^ 1) * hp1 + aa) * 2), ld_c(Y + (lane * hp1 + bb) * 2));
-      t = warp_sum_c(t);
-      if (lane == 0) st_c(acc_v + 2 * k, cscale(t, 0.5));
+      for (int i = 0; i < s; ++i) t = cadd(t, cmul(ld_c(Y + ((i ^ 1) * hp1 + aa) * 2), ld_c(Y + (i * hp1 + bb) * 2)));
+      st_c(acc_v + 2 * k, cscale(t, 0.5));
+    }
+    for (int k = 1; k <= n; ++k) {
+      const int aa = (k - 1) >> 1, bb = k - 1 - aa;
       if constexpr (CERT) {
         double vb = lane < s ? ru_mul(Ym[(lane ^ 1) * hp1 + aa], Ym[lane * hp1 + bb]) : 0.0;
         vb = warp_sum_ru(vb);
@@ -509,7 +518,9 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       const double sq2 = 1.4142135623730952;
       const double g64 = ru_mul(sq2, gamma_ru(64.0, kU));
       const double gy = ru_mul(sq2, gamma_ru((double)(s + 4), kU));
-      const double gv = ru_add(4.0 * kU, gamma_ru(8.0, kU));
+      // loop term: complex products (4u) summed sequentially over s rows
+      // (sqrt(2) gamma_{s+4} <= gamma_{2s+8} per component pair)
+      const double gv = ru_add(4.0 * kU, gamma_ru(2.0 * s + 8.0, kU));
       double ca[kHafMaxPow + 2], ph[kHafMaxPow + 2], ka[kHafMaxPow + 2];
       ca[0] = 0.0; ph[0] = 1.0; ca[1] = 0.0; ph[1] = 1.0;
       for (int a = 1; a <= h; ++a) {

@@ -30,6 +30,7 @@
 #include "haf_pt.cuh"
 #include "tor_lu.cuh"
 #include "tor_warp.cuh"
+#include "tor_warp_dd.cuh"
 
 namespace gbsb {
 
@@ -132,6 +133,23 @@ struct Plan {
 };
 
 
+// ------------------------------------------------------------------ tuned splits
+// Work-item split and block size per (function, binary64 or double-double tiers,
+// evaluated side), written by the autotuner through gbs_set_split; 0 = unset (the
+// planner's default).  Stored as value + 1.  The binary64 tiers (fp64, indicator,
+// certified) share one entry so their values stay bit-identical.
+constexpr int kTuneDims = 65;
+static std::atomic<int> g_tune_split[4][2][kTuneDims];
+static std::atomic<int> g_tune_warps[4][2][kTuneDims];
+int tuned_split(int fn, int tier, int dim) {  // also read by the allocation-free entry point
+  if (fn < 0 || fn > 3 || dim < 0 || dim >= kTuneDims) return -1;
+  return g_tune_split[fn][tier == kTierDD ? 1 : 0][dim].load() - 1;
+}
+static int tuned_warps(int fn, int tier, int dim) {
+  if (fn < 0 || fn > 3 || dim < 0 || dim >= kTuneDims) return 0;
+  return g_tune_warps[fn][tier == kTierDD ? 1 : 0][dim].load();
+}
+
 // Cost model (relative units) used only to order the queue heaviest-first.
 static double item_cost(int fn, int dim, unsigned long long count, int tier, int param) {
   double c;
@@ -145,7 +163,8 @@ static double item_cost(int fn, int dim, unsigned long long count, int tier, int
         c = (double)count * dim * dim * dim;
         break;
       }
-      c = tier == kTierDD ? (double)count * std::ldexp(1.0, n - param) * n * n
+      const int qd = n - std::min(n, 4);
+      c = tier == kTierDD ? 20.0 * (double)count * std::ldexp(1.0, qd - param) * 16.0 * (36.0 * qd + 900.0)
                           : (double)count * std::ldexp(1.0, q - param) * 32.0 * (36.0 * q + 1400.0);
       break;
     }
@@ -178,7 +197,9 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
       add(0, terms);
     } else {
       const int rcap = tier == kTierDD ? 6 : 10;
-      const int rlog = std::min(n - 1 - 5, rcap);
+      int rlog = std::min(n - 1 - 5, rcap);
+      const int tl = tuned_split(fn, tier, dim_eval);
+      if (tl >= 0) rlog = std::min(n - 1 - 5, tl);
       const unsigned long long cnt = 32ull << rlog;
       for (unsigned long long lo = 0; lo < terms; lo += cnt) add(lo, cnt);
       d.param = rlog;
@@ -187,7 +208,9 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     const int n = dim_eval / 2;
     const unsigned long long masks = 1ull << n;
     // masks per item: 2^7 (binary64 tiers) / 2^6 (double-double); smaller instances are one item
-    const int per = tier == kTierDD ? std::min(n, 6) : std::min(n, 7);
+    int per = tier == kTierDD ? std::min(n, 6) : std::min(n, 7);
+    const int tl = tuned_split(fn, tier, dim_eval);
+    if (tl >= 0) per = std::min(n, tl);
     const unsigned long long cnt = 1ull << per;
     for (unsigned long long lo = 0; lo < masks; lo += cnt) add(lo, std::min(cnt, masks - lo));
     P.haf_smax = std::max(P.haf_smax, dim_eval);
@@ -196,11 +219,13 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     const int per = std::min(n, 6);
     for (unsigned long long lo = 0; lo < (1ull << n); lo += (1ull << per)) add(lo, 1ull << per);
     d.param = -1;
-  } else if (tier == kTierDD) {  // tor, double-double: one lane per prefix pattern
+  } else if (tier == kTierDD) {  // tor, double-double: the warp walk, 16-subset tail
     const int n = dim_eval / 2;
-    const int g = std::max(std::min(n, 5), n - 7);
-    const unsigned long long pats = 1ull << g;
-    for (unsigned long long lo = 0; lo < pats; lo += 32) add(lo, std::min<unsigned long long>(32, pats - lo));
+    const int q = n - std::min(n, kTorTailDD);
+    int g = std::max(0, q - 6);  // 2^6 prefix leaves per item
+    const int tl = tuned_split(fn, tier, dim_eval);
+    if (tl >= 0) g = std::max(0, q - tl);
+    for (unsigned long long p = 0; p < (1ull << g); ++p) add(p, 1);
     d.param = g;
   } else {  // tor, binary64 tiers: one warp per prefix pattern over the first g prefix modes
     const int n = dim_eval / 2;
@@ -208,6 +233,8 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     // 2^9 leaves (x 32 tail subsets) per item, the same split for every binary64
     // tier so that the certified and indicator values are the fp64 value bit for bit
     int g = std::max(0, q - 9);
+    const int tl = tuned_split(fn, tier, dim_eval);  // log2 prefix leaves per item
+    if (tl >= 0) g = std::max(0, q - tl);
     if (split >= 0) g = std::min(q, std::max(g, split));
     for (unsigned long long p = 0; p < (1ull << g); ++p) add(p, 1);
     d.param = g;
@@ -225,7 +252,7 @@ static int ws_for_plan(const Plan& P) {
     int w = 0;
     if (fn == kFnPerm) w = 2 * d.dim * d.dim;
     else if (fn == kFnTor && !d.real_in) w = tor_lu_ws_doubles();
-    else if (fn == kFnTor) w = tier == kTierDD ? d.dim * d.dim : tor_w_layout(d.dim / 2, tier == kTierCert).total;
+    else if (fn == kFnTor) w = tier == kTierDD ? tor_d_layout(d.dim / 2).total : tor_w_layout(d.dim / 2, tier == kTierCert).total;
     else if (tier == kTierDD) w = haf_dd_layout(P.haf_smax).total;
     else w = haf_layout(P.haf_smax, tier == kTierCert).total;
     ws = std::max(ws, w);
@@ -275,6 +302,11 @@ struct gbs_session {
   std::vector<gbsb::cplx> plan_tval;
   size_t plan_ninst = 0;
   bool plan_ready = false;
+  // CUDA graph of the prepared plan's launch sequence (queue resets + one launch per
+  // group), captured on its second run and replayed afterwards; dropped with the plan
+  bool use_graphs = true;
+  int plan_runs = 0;
+  cudaGraphExec_t graph = nullptr;
   std::mutex mu;
 };
 
@@ -387,8 +419,15 @@ struct RunOpts {
 // group holds every haf / lhaf / tor request (persistent mixed queue); the
 // permanent gets one group per tier; per-size mode gives one group per
 // (func, tier, size) bucket.
+static void drop_graph(gbs_session* s) {
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  s->graph = nullptr;
+  s->plan_runs = 0;
+}
+
 static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpts& opt) {
   s->plan_ready = false;
+  drop_graph(s);
   s->groups.clear();
   const int B = (int)reqs.size();
   s->plan_B = B;
@@ -562,6 +601,10 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
     // families) so the SM packs as many warps as shared memory allows
     const size_t smem_per_warp = (size_t)P.ws_doubles * sizeof(double);
     int warps = smem_per_warp >= 8192 ? 1 : opt.warps;
+    if (opt.per_size && !P.insts.empty()) {  // a per-size bucket: the tuned block size, if any
+      const int tw = tuned_warps(P.insts[0].ft >> 2, P.insts[0].ft & 3, P.insts[0].dim);
+      if (tw > 0) warps = tw;
+    }
     while (warps > 1 && (size_t)warps * smem_per_warp > 200 * 1024) warps >>= 1;
     const int bps = occ_any(G.br, L, warps);
     if (bps <= 0) return fail(cudaErrorInvalidConfiguration, "work item kernel does not fit on an SM");
@@ -588,23 +631,51 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
 
 // Launch the prepared plan on `stream` (the session stream when null): reset the
 // queue heads and completion counters, then one kernel per group.
-static int plan_launch(gbs_session* s, cudaStream_t stream) {
-  if (!s->plan_ready) return fail(cudaErrorInvalidValue, "no prepared plan");
-  if (!stream) stream = s->stream;
+// The launch sequence of the prepared plan: queue resets + one launch per group.
+static cudaError_t plan_enqueue(gbs_session* s, cudaStream_t stream) {
   cudaError_t e = cudaSuccess;
   if (!s->groups.empty()) {
     e = cudaMemsetAsync(s->head.p, 0, 64 * s->groups.size(), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->done.p, 0, s->plan_ninst * sizeof(int), stream);
   }
-  if (e != cudaSuccess) return fail(e, "resetting the work queues");
-  cudaEventRecord(s->ev0, stream);
-  long long items = 0;
   for (auto& G : s->groups) {
+    if (e != cudaSuccess) break;
     e = launch_any(G.br, G.L, G.grid, G.warps, stream);
-    if (e != cudaSuccess) return fail(e, "launching the work item kernel");
-    items += G.nit;
   }
+  return e;
+}
+
+// Run the prepared plan on `stream`.  From the second run of a plan on (the first
+// run sets every kernel attribute), with graphs enabled, the sequence is captured
+// once into a CUDA graph and replayed: one graph launch per run.
+static int plan_launch(gbs_session* s, cudaStream_t stream, bool allow_graph = false) {
+  if (!s->plan_ready) return fail(cudaErrorInvalidValue, "no prepared plan");
+  if (!stream) stream = s->stream;
+  cudaError_t e = cudaSuccess;
+  long long items = 0;
+  for (auto& G : s->groups) items += G.nit;
+  const bool graph_now = allow_graph && s->use_graphs && !s->groups.empty() && s->plan_runs >= 1;
+  if (graph_now && !s->graph) {
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const cudaError_t e1 = plan_enqueue(s, stream);
+      e = cudaStreamEndCapture(stream, &g);
+      if (e == cudaSuccess) e = e1;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      s->graph = nullptr;
+      return fail(e, "capturing the plan's launch graph");
+    }
+  }
+  cudaEventRecord(s->ev0, stream);
+  if (graph_now) e = cudaGraphLaunch(s->graph, stream);
+  else e = plan_enqueue(s, stream);
+  if (e != cudaSuccess) return fail(e, "launching the work item kernel");
   cudaEventRecord(s->ev1, stream);
+  s->plan_runs += 1;
   s->last_launches = (int)s->groups.size();
   s->last_items = items;
   return 0;
@@ -696,6 +767,7 @@ static int session_open(gbs_session** out) {
 static void session_free(gbs_session* s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graph(s);
   for (DevBuf* b : {&s->mats, &s->meta, &s->part, &s->paux, &s->pst, &s->done, &s->head, &s->out, &s->aux, &s->st,
                     &s->gather})
     if (b->p) cudaFree(b->p);
@@ -990,7 +1062,35 @@ int gbs_queue_prepare(gbs_session* s, int B, const int* funcs, const int* tiers,
 int gbs_queue_run(gbs_session* s, void* stream) {
   if (!s) return fail(cudaErrorInvalidValue, "null session");
   std::lock_guard<std::mutex> lk(s->mu);
-  return plan_launch(s, (cudaStream_t)stream);
+  return plan_launch(s, (cudaStream_t)stream, true);
+}
+
+// Autotuner hooks: split = log2 of the work per item (haf / lhaf: subsets per item;
+// perm: Gray steps per lane; tor: prefix leaves per item, or subsets per lane in the
+// double-double tier); warps = block size of per-size launches; -1 / 0 = default.
+int gbs_set_split(int func, int tier, int dim, int split, int warps) {
+  if (func < 0 || func > 3 || tier < 0 || tier > 3 || dim < 0 || dim >= kTuneDims || split < -1 || split > 40 ||
+      warps < 0 || warps > 8)
+    return fail(cudaErrorInvalidValue, "gbs_set_split: argument out of range");
+  const int t = tier == kTierDD ? 1 : 0;
+  g_tune_split[func][t][dim].store(split + 1);
+  g_tune_warps[func][t][dim].store(warps);
+  return 0;
+}
+int gbs_get_split(int func, int tier, int dim, int* split, int* warps) {
+  if (func < 0 || func > 3 || tier < 0 || tier > 3 || dim < 0 || dim >= kTuneDims)
+    return fail(cudaErrorInvalidValue, "gbs_get_split: argument out of range");
+  if (split) *split = tuned_split(func, tier, dim);
+  if (warps) *warps = tuned_warps(func, tier, dim);
+  return 0;
+}
+
+int gbs_session_set_graphs(gbs_session* s, int enable) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->use_graphs = enable != 0;
+  if (!s->use_graphs) drop_graph(s);
+  return 0;
 }
 int gbs_queue_read(gbs_session* s, void* stream, double* out, double* aux, int* status) {
   if (!s || !out) return fail(cudaErrorInvalidValue, "null argument");

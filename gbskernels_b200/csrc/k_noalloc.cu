@@ -22,6 +22,8 @@
 
 namespace gbsb {
 
+int tuned_split(int fn, int tier, int dim);  // host_api.cu: the autotuner's split table
+
 // Fixed scratch: 4 MiB per device, 256-byte aligned.
 constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;
 // Limits that fit the scratch: items x 68 bytes + instances x 48 bytes + 256.
@@ -95,7 +97,9 @@ int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void*
     return (int)cudaMemcpyAsync(d_out, g_h_ones, (size_t)batch * 16, cudaMemcpyHostToDevice, st);
   }
   const int n = N / 2;
-  const int per = n < 7 ? n : 7;  // the planner's decomposition (bit-identical results)
+  int per = n < 7 ? n : 7;  // the planner's decomposition (bit-identical results)
+  const int tl = tuned_split(kFnHaf, kTierFp64, N);
+  if (tl >= 0) per = tl < n ? tl : n;
   const long long items_per = 1ll << (n - per);
   const long long nit = items_per * batch;
   if (batch > kNoAllocMaxInstances || nit > kNoAllocMaxItems) {

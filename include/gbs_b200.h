@@ -123,6 +123,18 @@ int gbs_queue_run(gbs_session* s, void* stream);
 int gbs_queue_read(gbs_session* s, void* stream, double* out, double* aux, int* status);
 /* kernel time (CUDA events), launches and work items of the session's last call */
 int gbs_session_last_stats(const gbs_session* s, double* kernel_ms, int* launches, long long* items);
+/* gbs_queue_run captures a prepared plan's launch sequence (queue resets + one
+ * launch per group) into a CUDA graph on its second run and replays the graph
+ * afterwards; enable = 0 turns that off for the session.  No reference counterpart
+ * (the reference launches each size bucket directly).                           */
+int gbs_session_set_graphs(gbs_session* s, int enable);
+/* Autotuner hooks (process-wide).  split = log2 of the work per item for
+ * (func, tier, evaluated side): haf / lhaf subsets per item, perm Gray steps per
+ * lane, tor prefix leaves per item (double-double: subsets per lane); -1 = the
+ * planner's default.  warps = block size of per-size launches (0 = default).  The
+ * binary64 tiers share one entry.  No reference counterpart.                     */
+int gbs_set_split(int func, int tier, int dim, int split, int warps);
+int gbs_get_split(int func, int tier, int dim, int* split, int* warps);
 
 /* ---- continuous-batching server (chain-rule sampler queries) -----------------
  * No reference counterpart (the reference's resident sampler session,

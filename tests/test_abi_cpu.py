@@ -108,3 +108,16 @@ def test_workspace_lifecycle_errors(G):
         ws.haf_batched([np.eye(2)])
     with pytest.raises(ValueError, match="unknown backend"):
         G.Workspace(backend="tpu")
+
+
+def test_tuned_split_table(lib):
+    import numpy as np
+    from gbskernels_b200 import _lib
+    s = np.zeros(1, np.int32)
+    w = np.zeros(1, np.int32)
+    assert lib.gbs_get_split(1, 0, 20, _lib.iptr(s), _lib.iptr(w)) == 0 and (s[0], w[0]) == (-1, 0)
+    assert lib.gbs_set_split(1, 3, 20, 6, 2) == 0  # certified shares the binary64 entry
+    assert lib.gbs_get_split(1, 0, 20, _lib.iptr(s), _lib.iptr(w)) == 0 and (s[0], w[0]) == (6, 2)
+    assert lib.gbs_get_split(1, 1, 20, _lib.iptr(s), _lib.iptr(w)) == 0 and s[0] == -1  # dd separate
+    assert lib.gbs_set_split(1, 0, 20, -1, 0) == 0
+    assert lib.gbs_set_split(9, 0, 20, 6, 0) != 0 and lib.gbs_set_split(1, 0, 99, 6, 0) != 0
