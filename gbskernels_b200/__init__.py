@@ -36,7 +36,7 @@ __all__ = [
 
 PRECISIONS = ("fp64", "ref", "dd", "auto", "certified")
 _FN = {"perm": 0, "haf": 1, "lhaf": 2, "tor": 3}
-_TIER = {"fp64": 0, "dd": 1, "kappa": 2, "certified": 3}
+_TIER = {"fp64": 0, "dd": 1, "kappa": 2, "certified": 3, "certified-dd": 4}
 _AUTO_KAPPA_MAX = 1e8  # gbskernels/__init__.py:240
 
 # Largest input side each kernel family supports (tor: 2n).
@@ -370,8 +370,8 @@ def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: b
     One instance split into at least ``2**groups`` prefix work items over the
     whole GPU (the warp-cooperative walk of the batched kernel, lifted to 32
     modes).  ``certified=True`` returns ``(value, diagnostics)`` with a rigorous
-    a-posteriori bound; ``dd=True`` (the reference's double-double certified
-    variant) is not provided and raises RuntimeError."""
+    a-posteriori bound; ``dd=True`` (implies certified) computes the value in
+    double-word arithmetic with the same kind of bound (tier ``"certified-dd"``)."""
     A = np.asarray(O)
     if np.iscomplexobj(A):
         if np.any(np.imag(A) != 0):
@@ -393,14 +393,9 @@ def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: b
     lib = _lib.load()
     v = np.zeros(1)
     e = np.zeros(1)
-    if dd:
-        # the reference's double-double certified single-large kernel has no
-        # counterpart here; like the reference without it, this is a RuntimeError
-        raise RuntimeError("tor_single(certified-dd) is not in this build; use certified=True "
-                           "(binary64 value with a rigorous a-posteriori bound)")
-    if certified:
-        tier = "certified-fp64"
-        name = "gbs_tor_single_certified_host"
+    if certified or dd:
+        tier = "certified-dd" if dd else "certified-fp64"
+        name = "gbs_tor_single_ddcertified_host" if dd else "gbs_tor_single_certified_host"
         fn = getattr(lib, name, None)
         if fn is None:
             raise RuntimeError(f"tor_single({tier}) is not in this build")

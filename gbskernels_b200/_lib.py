@@ -40,6 +40,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     # single-large torontonian
     "gbs_tor_recursive_single_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
     "gbs_tor_single_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "gbs_tor_single_ddcertified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
     # sessions
     "gbs_session_open": ([ctypes.POINTER(_vp)], ctypes.c_int),
     "gbs_session_close": ([_vp], ctypes.c_int),

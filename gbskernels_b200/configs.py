@@ -23,7 +23,7 @@ import numpy as np
 from . import Workspace, _lib, _pack, workloads
 
 _FN = {"perm": 0, "haf": 1, "lhaf": 2, "tor": 3}
-_TIER = {"fp64": 0, "dd": 1, "kappa": 2, "certified": 3}
+_TIER = {"fp64": 0, "dd": 1, "kappa": 2, "certified": 3, "certified-dd": 4}
 
 
 def run(func: str, mats: list, tier: str = "fp64", per_size: bool = False, reps: int = 1) -> dict:
@@ -47,7 +47,7 @@ def run(func: str, mats: list, tier: str = "fp64", per_size: bool = False, reps:
     res = {"func": func, "tier": tier, "batch": B, "mode": "per-size" if per_size else "persistent",
            "kernel_ms": stats["kernel_ms"], "instances_per_s": B / stats["kernel_ms"] * 1e3,
            "launches": stats["launches"], "items": stats["items"], "status_ok": int((st == 0).sum())}
-    if tier == "certified":
+    if tier in ("certified", "certified-dd"):
         rel = aux / np.maximum(np.abs(out), 1e-300)
         res["rel_bound_median"] = float(np.median(rel))
         res["rel_bound_max"] = float(np.max(rel))

@@ -183,7 +183,7 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
     }
     return r;
   }
-  if constexpr (TIER != kTierDD) {
+  if constexpr (TIER != kTierDD && TIER != kTierCertDD) {
     // binary64 tiers: warp-cooperative prefix walk with the 32-subset register tail
     // (tor_warp.cuh); one work item = w.count prefix patterns over the first d.param
     // prefix modes, walked one after another by the whole warp
@@ -221,18 +221,39 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
     __syncwarp();
     return r;
   } else {
-    // double-double tier: the same walk in double-word arithmetic with a 16-subset
-    // tail (tor_warp_dd.cuh); one work item = w.count prefix patterns
-    const TorDLayout Lw = tor_d_layout(n);
+    // double-double tiers: the same walk in double-word arithmetic with a 16-subset
+    // tail (tor_warp_dd.cuh); one work item = w.count prefix patterns.  The certified
+    // tier adds the radius (same value bit for bit).
+    constexpr bool CERT = TIER == kTierCertDD;
+    const TorDLayout Lw = tor_d_layout(n, CERT);
+    double* rho = ws + Lw.rho_off;
+    bool proved = true;
+    if (CERT) {
+      double dmin2 = 0.0;
+      const double sigma = tor_cert_sigma(Oc, n, ws + Lw.col_off, lane, dmin2);
+      proved = sigma > 0.0;
+      tor_cert_rho_dd(sigma, dmin2, n, rho, lane);
+    }
     dd val = dd_make(0.0);
+    double aux = 0.0;
     bool ok = true;
-    for (unsigned long long p = 0; p < w.count; ++p) {
-      dd t = dd_make(0.0);
-      ok = tor_dd_item(Oc, n, d.param, (uint32_t)(w.lo + p), ws, Lw, lane, t) && ok;
-      val = p == 0 ? t : dd_add(val, t);
+    if (proved) {
+      for (unsigned long long p = 0; p < w.count; ++p) {
+        dd t = dd_make(0.0);
+        double a = 0.0;
+        ok = tor_dd_item<CERT>(Oc, n, d.param, (uint32_t)(w.lo + p), ws, Lw, rho, lane, t, a) && ok;
+        if (p == 0) {
+          val = t;
+          aux = a;
+        } else {
+          val = dd_add(val, t);
+          if (CERT) aux = ru_add(ru_add(aux, a), ru_add(ru_mul(4.0 * kU * kU, fabs(val.hi)), kUfl));
+        }
+      }
     }
     r.val = ddc{val, dd_make(0.0)};
-    if (!ok) r.st = kStOffDomain;
+    r.aux = aux;
+    if (!proved || !ok) r.st = CERT ? kStUncertified : kStOffDomain;
     __syncwarp();
     return r;
   }
@@ -264,6 +285,7 @@ __device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstD
     GBSB_BR(kFnHaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, false, ws, P.haf_smax, lane)))
     GBSB_BR(kFnLhaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, true, ws, P.haf_smax, lane)))
     GBSB_BR(kFnTor, kTierCert, (tor_item<kTierCert>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnTor, kTierCertDD, (tor_item<kTierCertDD>(P.mats, d, w, ws, lane)))
 #undef GBSB_BR
     default:
       break;
@@ -301,7 +323,7 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
       __threadfence();
       // Deterministic reduction: lane l sums items l, l+32, ... in order, then a
       // fixed butterfly combines the lanes.  Partials are read through L2.
-      const bool cert = (d.ft & 3) == kTierCert;
+      const bool cert = tier_certified(ft_tier(d.ft));
       ddc acc = ddc{dd_make(0.0), dd_make(0.0)};
       double aux = 0.0, mag = 0.0;
       int st = kStOk;
@@ -321,7 +343,7 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
       for (int m = 16; m > 0; m >>= 1) st = max(st, __shfl_xor_sync(0xffffffffu, st, m));
       if (lane == 0) {
         cplx v = ddc_to_c(acc);
-        const int fn = d.ft >> 2;
+        const int fn = ft_fn(d.ft);
         if (fn == kFnPerm && d.dim > 0) {
           const double sc = ldexp(1.0, -(d.dim - 1));  // 1 / 2^(n-1), exact
           v = cscale(v, sc);

@@ -15,10 +15,13 @@ namespace gbsb {
 
 // function codes (the reference's Session numbering, core/host_api.cu:472-480)
 enum : int { kFnPerm = 0, kFnHaf = 1, kFnLhaf = 2, kFnTor = 3 };
-// tier codes
-enum : int { kTierFp64 = 0, kTierDD = 1, kTierKappa = 2, kTierCert = 3 };
+// tier codes (kTierCertDD: double-double value + rigorous bound, torontonian only)
+enum : int { kTierFp64 = 0, kTierDD = 1, kTierKappa = 2, kTierCert = 3, kTierCertDD = 4 };
 
-__host__ __device__ constexpr int ft_code(int fn, int tier) { return fn * 4 + tier; }
+__host__ __device__ constexpr int ft_code(int fn, int tier) { return fn * 8 + tier; }
+__host__ __device__ constexpr int ft_fn(int ft) { return ft >> 3; }
+__host__ __device__ constexpr int ft_tier(int ft) { return ft & 7; }
+__host__ __device__ constexpr bool tier_certified(int tier) { return tier == kTierCert || tier == kTierCertDD; }
 
 struct InstDesc {       // 32 bytes
   long long off;        // offset (in doubles) of the matrix in the packed input buffer
@@ -46,7 +49,8 @@ constexpr unsigned kBrServe = kBrHafLhafFp64 | br1(kFnTor, kTierFp64) | br1(kFnH
                               br1(kFnLhaf, kTierKappa) | br1(kFnTor, kTierKappa) | br1(kFnHaf, kTierCert) |
                               br1(kFnLhaf, kTierCert) | br1(kFnTor, kTierCert);
 // haf / lhaf / tor in every tier
-constexpr unsigned kBrMixed = kBrServe | br1(kFnHaf, kTierDD) | br1(kFnLhaf, kTierDD) | br1(kFnTor, kTierDD);
+constexpr unsigned kBrMixed = kBrServe | br1(kFnHaf, kTierDD) | br1(kFnLhaf, kTierDD) | br1(kFnTor, kTierDD) |
+                              br1(kFnTor, kTierCertDD);
 
 // Device buffers of one launch.
 struct ItemLaunch {

@@ -143,11 +143,11 @@ static std::atomic<int> g_tune_split[4][2][kTuneDims];
 static std::atomic<int> g_tune_warps[4][2][kTuneDims];
 int tuned_split(int fn, int tier, int dim) {  // also read by the allocation-free entry point
   if (fn < 0 || fn > 3 || dim < 0 || dim >= kTuneDims) return -1;
-  return g_tune_split[fn][tier == kTierDD ? 1 : 0][dim].load() - 1;
+  return g_tune_split[fn][(tier == kTierDD || tier == kTierCertDD) ? 1 : 0][dim].load() - 1;
 }
 static int tuned_warps(int fn, int tier, int dim) {
   if (fn < 0 || fn > 3 || dim < 0 || dim >= kTuneDims) return 0;
-  return g_tune_warps[fn][tier == kTierDD ? 1 : 0][dim].load();
+  return g_tune_warps[fn][(tier == kTierDD || tier == kTierCertDD) ? 1 : 0][dim].load();
 }
 
 // Cost model (relative units) used only to order the queue heaviest-first.
@@ -164,7 +164,7 @@ static double item_cost(int fn, int dim, unsigned long long count, int tier, int
         break;
       }
       const int qd = n - std::min(n, 4);
-      c = tier == kTierDD ? 20.0 * (double)count * std::ldexp(1.0, qd - param) * 16.0 * (36.0 * qd + 900.0)
+      c = (tier == kTierDD || tier == kTierCertDD) ? 20.0 * (double)count * std::ldexp(1.0, qd - param) * 16.0 * (36.0 * qd + 900.0)
                           : (double)count * std::ldexp(1.0, q - param) * 32.0 * (36.0 * q + 1400.0);
       break;
     }
@@ -219,7 +219,7 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     const int per = std::min(n, 6);
     for (unsigned long long lo = 0; lo < (1ull << n); lo += (1ull << per)) add(lo, 1ull << per);
     d.param = -1;
-  } else if (tier == kTierDD) {  // tor, double-double: the warp walk, 16-subset tail
+  } else if (tier == kTierDD || tier == kTierCertDD) {  // tor, double-double: the warp walk, 16-subset tail
     const int n = dim_eval / 2;
     const int q = n - std::min(n, kTorTailDD);
     int g = std::max(0, q - 6);  // 2^6 prefix leaves per item
@@ -248,11 +248,12 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
 static int ws_for_plan(const Plan& P) {
   int ws = 2;
   for (const InstDesc& d : P.insts) {
-    const int fn = d.ft >> 2, tier = d.ft & 3;
+    const int fn = ft_fn(d.ft), tier = ft_tier(d.ft);
     int w = 0;
     if (fn == kFnPerm) w = 2 * d.dim * d.dim;
     else if (fn == kFnTor && !d.real_in) w = tor_lu_ws_doubles();
-    else if (fn == kFnTor) w = tier == kTierDD ? tor_d_layout(d.dim / 2).total : tor_w_layout(d.dim / 2, tier == kTierCert).total;
+    else if (fn == kFnTor && (tier == kTierDD || tier == kTierCertDD)) w = tor_d_layout(d.dim / 2, tier == kTierCertDD).total;
+    else if (fn == kFnTor) w = tor_w_layout(d.dim / 2, tier == kTierCert).total;
     else if (tier == kTierDD) w = haf_dd_layout(P.haf_smax).total;
     else w = haf_layout(P.haf_smax, tier == kTierCert).total;
     ws = std::max(ws, w);
@@ -349,7 +350,9 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
   *trivial = false;
   *real_in = false;
   if (r.dim < 0) return fail(cudaErrorInvalidValue, "negative matrix dimension");
-  if (r.tier < 0 || r.tier > 3) return fail(cudaErrorInvalidValue, "unsupported precision tier");
+  if (r.tier < 0 || r.tier > 4) return fail(cudaErrorInvalidValue, "unsupported precision tier");
+  if (r.tier == kTierCertDD && r.fn != kFnTor)
+    return fail(cudaErrorNotSupported, "the certified double-double tier is provided for the torontonian only");
   switch (r.fn) {
     case kFnPerm:
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
@@ -389,7 +392,7 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
       }
       if (!re) {
         // complex O: subset LU determinants, binary64 tiers, the reference's GPU cap
-        if (r.tier == kTierDD || r.tier == kTierCert || r.single)
+        if (r.tier == kTierDD || r.tier == kTierCert || r.tier == kTierCertDD || r.single)
           return fail(cudaErrorNotSupported,
                       "torontonian: complex O is supported in the fp64 tier only (the double-double, "
                       "certified and single-large paths are real-domain)");
@@ -495,7 +498,7 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
       std::vector<double> c(ni);
       for (int k = 0; k < ni; ++k) {
         const InstDesc& d = P.insts[k];
-        c[k] = item_cost(d.ft >> 2, d.dim, P.items[d.item0].count, d.ft & 3, d.param);
+        c[k] = item_cost(ft_fn(d.ft), d.dim, P.items[d.item0].count, ft_tier(d.ft), d.param);
       }
       std::stable_sort(inst_order.begin(), inst_order.end(), [&](int a, int b) { return c[a] > c[b]; });
     }
@@ -602,7 +605,7 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
     const size_t smem_per_warp = (size_t)P.ws_doubles * sizeof(double);
     int warps = smem_per_warp >= 8192 ? 1 : opt.warps;
     if (opt.per_size && !P.insts.empty()) {  // a per-size bucket: the tuned block size, if any
-      const int tw = tuned_warps(P.insts[0].ft >> 2, P.insts[0].ft & 3, P.insts[0].dim);
+      const int tw = tuned_warps(ft_fn(P.insts[0].ft), ft_tier(P.insts[0].ft), P.insts[0].dim);
       if (tw > 0) warps = tw;
     }
     while (warps > 1 && (size_t)warps * smem_per_warp > 200 * 1024) warps >>= 1;
@@ -885,11 +888,11 @@ int gbs_lhaf_kappa_host(const double* m, int N, int b, double* o, double* a) { r
 int gbs_tor_kappa_host(const double* m, int n, int b, double* o, double* a) { return one_shot(kFnTor, kTierKappa, m, 2 * n, b, o, a); }
 
 // ---- certified tier: value + rigorous bound (core/host_api.cu:248-262) ---------
-static int one_shot_cert(int fn, const double* m, int dim, int b, double* o, double* bound) {
+static int one_shot_cert(int fn, const double* m, int dim, int b, double* o, double* bound, int tier = kTierCert) {
   if (b > 0 && !bound) return fail(cudaErrorInvalidValue, "null bound buffer");
   for (size_t i = 0; i < 2ull * (size_t)dim * dim * (size_t)std::max(b, 0); ++i)
     if (!std::isfinite(m[i])) return fail(cudaErrorInvalidValue, "certified evaluation requires finite input");
-  int rc = one_shot(fn, kTierCert, m, dim, b, o, bound);
+  int rc = one_shot(fn, tier, m, dim, b, o, bound);
   if (rc == 0)
     for (int i = 0; i < b; ++i)
       if (std::isnan(o[2 * i])) bound[i] = INFINITY;
@@ -899,13 +902,18 @@ int gbs_perm_certified_host(const double* m, int n, int b, double* o, double* e)
 int gbs_haf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnHaf, m, N, b, o, e); }
 int gbs_lhaf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnLhaf, m, N, b, o, e); }
 int gbs_tor_certified_host(const double* m, int n, int b, double* o, double* e) { return one_shot_cert(kFnTor, m, 2 * n, b, o, e); }
+// certified double-double torontonian: double-word value (returned rounded to
+// binary64) + rigorous bound, the rung above the binary64 certificate
+int gbs_tor_dd_certified_host(const double* m, int n, int b, double* o, double* e) {
+  return one_shot_cert(kFnTor, m, 2 * n, b, o, e, kTierCertDD);
+}
 
 // ---- single-large torontonian (core/host_api.cu:270-352) ---------------------
 // Real (2n x 2n) O, n <= 32, evaluated as ONE instance split into at least 2^g
 // prefix work items over the whole GPU.  Off the physical domain the value is NaN
 // (and the bound +inf); the certified variant returns the a-posteriori bound.
 static int tor_single(int tier, const double* O, int n, int g, double* out, double* bound) {
-  if (!O || !out || (tier == kTierCert && !bound)) return fail(cudaErrorInvalidValue, "null pointer");
+  if (!O || !out || (tier_certified(tier) && !bound)) return fail(cudaErrorInvalidValue, "null pointer");
   if (n < 0 || n > kTorSingleCapModes) return fail(cudaErrorInvalidValue, "single-large torontonian: n must be in [0, 32]");
   if (g < 0 || g > n) return fail(cudaErrorInvalidValue, "single-large torontonian: groups must be in [0, n]");
   const int dim = 2 * n;
@@ -942,6 +950,9 @@ int gbs_tor_recursive_single_host(const double* O, int n, int g, double* out) {
 }
 int gbs_tor_single_certified_host(const double* O, int n, int g, double* out, double* bound) {
   return tor_single(kTierCert, O, n, g, out, bound);
+}
+int gbs_tor_single_ddcertified_host(const double* O, int n, int g, double* out, double* bound) {
+  return tor_single(kTierCertDD, O, n, g, out, bound);
 }
 
 // ---- auto tier on the device (gbskernels/__init__.py:272-297) ----------------
@@ -1069,16 +1080,16 @@ int gbs_queue_run(gbs_session* s, void* stream) {
 // perm: Gray steps per lane; tor: prefix leaves per item, or subsets per lane in the
 // double-double tier); warps = block size of per-size launches; -1 / 0 = default.
 int gbs_set_split(int func, int tier, int dim, int split, int warps) {
-  if (func < 0 || func > 3 || tier < 0 || tier > 3 || dim < 0 || dim >= kTuneDims || split < -1 || split > 40 ||
+  if (func < 0 || func > 3 || tier < 0 || tier > 4 || dim < 0 || dim >= kTuneDims || split < -1 || split > 40 ||
       warps < 0 || warps > 8)
     return fail(cudaErrorInvalidValue, "gbs_set_split: argument out of range");
-  const int t = tier == kTierDD ? 1 : 0;
+  const int t = (tier == kTierDD || tier == kTierCertDD) ? 1 : 0;
   g_tune_split[func][t][dim].store(split + 1);
   g_tune_warps[func][t][dim].store(warps);
   return 0;
 }
 int gbs_get_split(int func, int tier, int dim, int* split, int* warps) {
-  if (func < 0 || func > 3 || tier < 0 || tier > 3 || dim < 0 || dim >= kTuneDims)
+  if (func < 0 || func > 3 || tier < 0 || tier > 4 || dim < 0 || dim >= kTuneDims)
     return fail(cudaErrorInvalidValue, "gbs_get_split: argument out of range");
   if (split) *split = tuned_split(func, tier, dim);
   if (warps) *warps = tuned_warps(func, tier, dim);

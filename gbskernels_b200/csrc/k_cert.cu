@@ -3,6 +3,7 @@
 #include "gbs_items.cuh"
 
 namespace gbsb {
-#define GBSB_LIST_CERT(X) X(br1(kFnHaf, kTierCert)) X(br1(kFnLhaf, kTierCert)) X(br1(kFnTor, kTierCert))
+#define GBSB_LIST_CERT(X) X(br1(kFnHaf, kTierCert)) X(br1(kFnLhaf, kTierCert)) X(br1(kFnTor, kTierCert)) \
+  X(br1(kFnTor, kTierCertDD))
 GBSB_DEFINE_GROUP(cert, GBSB_LIST_CERT)
 }  // namespace gbsb

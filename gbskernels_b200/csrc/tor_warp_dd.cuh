@@ -11,7 +11,24 @@
 // modes read from a packed identity, pivot reciprocal 0) and the signed terms
 // 1 / sqrt(det(M_S) det(Z_T')) are summed by a butterfly in double-word.
 // Pivot reciprocals 1 / sqrt(s) are one Newton step from the binary64 rsqrt seed:
-// y = y0 + y0 (1 - s y0^2) / 2 in double-word.
+// y = y0 + y0 (1 - s y0^2) / 2 in double-word.  The diagonal 1 - O_ii is formed
+// exactly (TwoSum), so M enters the walk without rounding.
+//
+// Certified double-double tier (kTierCertDD): the same walk (the value equals the
+// dd tier's bit for bit) with the a-posteriori radius of tor_warp.cuh re-derived for
+// double-word operations.  Per-operation relative error bounds (u = 2^-53):
+//   dd_add (the accurate double-word sum, Joldes-Muller-Popescu 2017, Alg. 6): 3u^2;
+//   dd_mul (TwoProd of the heads, both cross terms by FMA into the tail, Fast2Sum):
+//     error = xl*yh*d3 + (xh*yl + e1)(d2 + d3 + d2*d3) - xl*yl, at most 6u^2 + O(u^3)
+//     relative (|xl| <= u|xh|, |yl| <= u|yh|, |e1| <= u|xh*yh|); charged 7u^2;
+//   dd_mul_d: 2u^2 + O(u^3), charged 3u^2;
+//   dd_rsqrt: the Newton step leaves (3/2) e0^2 of the seed's relative error e0 <= 4u
+//     (rsqrt taken as 2 ulp) plus the roundings of its four operations: charged 40u^2.
+// Every factor entry is an inner product of <= m terms, each a dd_mul and a dd_add,
+// plus one scaling; the diagonal carries (1 + 40u^2)^2 from the pivot reciprocal:
+// gamma_{2m+16}(7u^2) covers all of it.  With sigma from the same binary64 eigenvalue
+// proof, rho_m follows as in tor_warp.cuh but evaluated as small quantities (1 + rho
+// is not representable in binary64): tor_cert_rho_dd.
 #pragma once
 
 #include "gbs_common.cuh"
@@ -24,13 +41,13 @@ constexpr int kTorTDdd = 2 * kTorTailDD;                  // 8 tail rows
 constexpr int kTorZEdd = kTorTDdd * (kTorTDdd + 1) / 2;  // 36 packed entries
 
 struct TorDLayout {
-  int col_off, inv_off, zd_off, det_off, gidx_off, id_off, total;  // in doubles
+  int col_off, inv_off, zd_off, det_off, gidx_off, id_off, rho_off, total;  // in doubles
 };
 
 // column u holds (rows - u) prefix slots + 8 tail slots, each a double-word
 __host__ __device__ inline int tor_col_base_dd(int u, int rows) { return u * (rows + kTorTDdd) - (u * (u - 1)) / 2; }
 
-__host__ __device__ inline TorDLayout tor_d_layout(int kmax) {
+__host__ __device__ inline TorDLayout tor_d_layout(int kmax, bool cert = false) {
   TorDLayout Lw;
   const int q = kmax > kTorTailDD ? kmax - kTorTailDD : 0;
   const int rows = 2 * q;
@@ -38,11 +55,22 @@ __host__ __device__ inline TorDLayout tor_d_layout(int kmax) {
   Lw.inv_off = Lw.col_off + 2 * (tor_col_base_dd(rows, rows) + 1);
   Lw.zd_off = Lw.inv_off + 2 * (rows + 1);
   Lw.det_off = Lw.zd_off + 2 * (q + 1) * kTorZEdd;
+  if (cert) {  // the eigenvalue proof factors a packed 2k x 2k matrix (+ 2k scalings) here
+    const int need = (2 * kmax) * (2 * kmax + 1) / 2 + 2 * kmax + 8;
+    if (Lw.det_off < need) Lw.det_off = (need + 1) & ~1;
+  }
   Lw.gidx_off = Lw.det_off + 2 * (q + 2);
   Lw.id_off = (Lw.gidx_off + (rows + 2) / 2 + 2) & ~1;  // 16-byte aligned double-words
-  Lw.total = Lw.id_off + 2 * kTorZEdd;
+  Lw.rho_off = Lw.id_off + 2 * kTorZEdd;
+  Lw.total = Lw.rho_off + (cert ? 2 * kmax + 2 : 0);
   Lw.total = (Lw.total + 3) & ~3;
   return Lw;
+}
+
+// entry of M = I - O as a double-word (the diagonal 1 - O_ii exact by TwoSum)
+__device__ __forceinline__ dd tor_m_dd(const double* __restrict__ Oc, int dim, int a, int b) {
+  const double o = Oc[2 * (a * dim + b)];
+  return a == b ? dd_add_d(dd_make(1.0), -o) : dd_make(-o);
 }
 
 __device__ __forceinline__ dd ld_dd(const double* p) {
@@ -96,16 +124,16 @@ __device__ __forceinline__ bool tor_d_append(const double* __restrict__ Oc, int 
     off[h] = x < R0 ? x : rows + (x - R0);
     if (x < R0) {
       const int gc = gidx[x];
-      a[h] = dd_make(tor_m(Oc, dim, gR0, gc));
-      b[h] = dd_make(tor_m(Oc, dim, gR1, gc));
+      a[h] = tor_m_dd(Oc, dim, gR0, gc);
+      b[h] = tor_m_dd(Oc, dim, gR1, gc);
     } else if (x < nx) {
       const int gT = tor_tail_g_dd(x - R0, q, k);
-      a[h] = dd_make(tor_m(Oc, dim, gR0, gT));
-      b[h] = dd_make(tor_m(Oc, dim, gR1, gT));
+      a[h] = tor_m_dd(Oc, dim, gR0, gT);
+      b[h] = tor_m_dd(Oc, dim, gR1, gT);
     }
   }
-  dd d00 = dd_make(tor_m(Oc, dim, gR0, gR0)), d10 = dd_make(tor_m(Oc, dim, gR1, gR0));
-  dd d11 = dd_make(tor_m(Oc, dim, gR1, gR1));
+  dd d00 = tor_m_dd(Oc, dim, gR0, gR0), d10 = tor_m_dd(Oc, dim, gR1, gR0);
+  dd d11 = tor_m_dd(Oc, dim, gR1, gR1);
   double* cv = col;
   auto step = [&](int v, dd av, dd bv) {
     const dd iv = ld_dd(inv + 2 * v);
@@ -183,8 +211,9 @@ __device__ __forceinline__ bool tor_d_append(const double* __restrict__ Oc, int 
 
 // One prefix leaf: lanes 0..2^r-1 factor their tail subset; returns the signed term.
 __device__ __forceinline__ dd tor_d_leaf(const double* zc, const double* zid, int r, int c, int k, dd detc, int lane,
-                                         bool& ok) {
+                                         bool& ok, int& m) {
   dd term = dd_make(0.0);
+  m = 0;
   if (lane < (1 << r)) {
     const int td = 2 * r;
     dd Lz[kTorZEdd];
@@ -213,16 +242,57 @@ __device__ __forceinline__ dd tor_d_leaf(const double* zc, const double* zid, in
       }
     }
     const int nin = __popc(lane);
+    m = 2 * (c + nin);
     const dd t = dd_rsqrt(dd_mul(detc, det));
     term = ((k - c - nin) & 1) ? dd_neg(t) : t;
   }
   return term;
 }
 
+// rho_m for m = 0..2k in double-double (see the header): all terms are small, so the
+// bound is assembled as small quantities in upward rounding,
+//   Up - 1 <= x + y + x y,  x = (gp + m eta) / (2 (1 - m eta)),  y = (m er + er) / (1 - m er - er)
+//   1 - Lo <= z/2 + z^2/2 + m er + er,  z = gp + m eta
+// (sqrt(1 + w) <= 1 + w/2; sqrt(1 - w) >= 1 - w/2 - w^2/2 for w <= 1/2).
+static __device__ __noinline__ void tor_cert_rho_dd(double sigma, double dmin2, int k, double* rho, int lane) {
+  const double u2 = 7.0 * kU * kU;
+  const double er = 40.0 * kU * kU;
+  for (int m = lane; m <= 2 * k; m += 32) {
+    double out;
+    if (m == 0) {
+      out = 0.0;
+    } else if (!(sigma > 0.0) || !(dmin2 > 0.0)) {
+      out = INFINITY;
+    } else {
+      const double md = (double)m;
+      const double g = gamma_ru(2.0 * md + 16.0, u2);
+      double cm = ru_div(g, rd_sub(1.0, g));
+      cm = ru_div(cm, __dmul_rd(rd_sub(1.0, kU), rd_sub(1.0, kU)));
+      cm = ru_add(cm, ru_div(ru_mul(2.0 * md + 16.0, 16.0 * kUfl), dmin2));
+      const double meta = ru_mul(md, ru_div(ru_mul(md, cm), sigma));
+      const double gp = gamma_ru(md + 1.0, u2);
+      const double mer = ru_add(ru_mul(md, er), er);
+      if (!(meta < 0.25) || !(mer < 0.25)) {
+        out = INFINITY;
+      } else {
+        const double z = ru_add(gp, meta);
+        const double x = ru_div(z, ru_mul(2.0, rd_sub(1.0, meta)));
+        const double y = ru_div(mer, rd_sub(1.0, mer));
+        const double up = ru_add(ru_add(x, y), ru_mul(x, y));
+        const double lo = ru_add(ru_add(ru_mul(0.5, z), ru_mul(0.5, ru_mul(z, z))), mer);
+        out = fmax(up, lo);
+      }
+    }
+    rho[m] = out;
+  }
+  __syncwarp();
+}
+
 // One work item: prefix pattern `pat` over the first g walked modes, then every
 // subset of the walked modes [g, q) with its 2^r tail subsets.
+template <bool CERT>
 static __device__ bool tor_dd_item(const double* __restrict__ Oc, int k, int g, uint32_t pat, double* ws,
-                                   const TorDLayout& Lw, int lane, dd& total) {
+                                   const TorDLayout& Lw, const double* rho, int lane, dd& total, double& aux) {
   const int dim = 2 * k;
   const int r = k < kTorTailDD ? k : kTorTailDD;
   const int q = k - r;
@@ -235,7 +305,7 @@ static __device__ bool tor_dd_item(const double* __restrict__ Oc, int k, int g, 
   for (int e = lane; e < kTorZEdd; e += 32) {
     int i, jj;
     tor_tri_ij(e, i, jj);
-    st_dd(zd + 2 * e, dd_make((i < 2 * r) ? tor_m(Oc, dim, tor_tail_g_dd(i, q, k), tor_tail_g_dd(jj, q, k)) : 0.0));
+    st_dd(zd + 2 * e, (i < 2 * r) ? tor_m_dd(Oc, dim, tor_tail_g_dd(i, q, k), tor_tail_g_dd(jj, q, k)) : dd_make(0.0));
     st_dd(zid + 2 * e, dd_make(i == jj ? 1.0 : 0.0));
   }
   if (lane == 0) st_dd(detat, dd_make(1.0));
@@ -252,6 +322,8 @@ static __device__ bool tor_dd_item(const double* __restrict__ Oc, int k, int g, 
     }
   const int pc = count;
   dd sum = dd_make(0.0);
+  double srad = 0.0;
+  constexpr double kU2x4 = 4.0 * kU * kU;  // bound of one dd_add, relative, with slack
   const int rp = q - g;
   const uint64_t nT = 1ull << rp;
   for (uint64_t Tm = 0; Tm < nT; ++Tm) {
@@ -262,10 +334,27 @@ static __device__ bool tor_dd_item(const double* __restrict__ Oc, int k, int g, 
       ok = tor_d_append(Oc, k, q, r, jz, count, col, inv, zd, detat, gidx, lane, zi, zj) && ok;
       ++count;
     }
-    const dd t = tor_d_leaf(zd + 2 * count * kTorZEdd, zid, r, count, k, ld_dd(detat + 2 * count), lane, ok);
-    sum = dd_add(sum, warp_sum_dd(t));
+    int m = 0;
+    const dd t = tor_d_leaf(zd + 2 * count * kTorZEdd, zid, r, count, k, ld_dd(detat + 2 * count), lane, ok, m);
+    if (CERT) {
+      // ball butterfly: the value operations are those of warp_sum_dd
+      dd v = t;
+      double rr = (t.hi != 0.0) ? ru_add(ru_mul(ru_mul(fabs(t.hi), 1.0 + 4.0 * kU), rho[m]), kUfl) : 0.0;
+#pragma unroll
+      for (int mm = 16; mm > 0; mm >>= 1) {
+        const dd ov{shfl_xor_d(v.hi, mm), shfl_xor_d(v.lo, mm)};
+        const double orr = shfl_xor_d(rr, mm);
+        v = dd_add(v, ov);
+        rr = ru_add(ru_add(rr, orr), ru_add(ru_mul(kU2x4, fabs(v.hi)), kUfl));
+      }
+      sum = dd_add(sum, v);
+      srad = ru_add(ru_add(srad, rr), ru_add(ru_mul(kU2x4, fabs(sum.hi)), kUfl));
+    } else {
+      sum = dd_add(sum, warp_sum_dd(t));
+    }
   }
   total = sum;
+  aux = srad;
   return __all_sync(0xffffffffu, ok);
 }
 

@@ -58,6 +58,12 @@ int gbs_perm_certified_host(const double* mats, int n, int batch, double* out, d
 int gbs_haf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
 int gbs_lhaf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
 int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, double* bound);
+/* certified double-double torontonian (real O, 24 modes batched): the value is
+ * computed in double-word arithmetic (returned rounded to binary64) and the bound
+ * is rigorous; the rung of the certified ladder above gbs_tor_certified_host.
+ * reference counterpart: the certified-dd rung of gbskernels/__init__.py:410-425
+ * (its batched dd-certified kernels cover perm / haf, core/host_api.cu:263-268).  */
+int gbs_tor_dd_certified_host(const double* mats, int n, int batch, double* out, double* bound);
 
 /* ---- single-large torontonian ----------------------------------------------
  * reference: core/host_api.cu:270-298 (gbs_tor_recursive_single_host) and :300-352
@@ -66,10 +72,12 @@ int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, do
  * split into at least 2^g prefix work items across the GPU (g in [0, n], the
  * reference's `groups`; the planner may split further).  Off the physical domain
  * (a non-SPD minor of I - O) *out is NaN and *bound +inf.  The certified bound is
- * rigorous: |*out - tor(O)| <= *bound.  The reference's double-double certified
- * single-large variant (gbs_tor_single_ddcertified_host) is not provided.        */
+ * rigorous: |*out - tor(O)| <= *bound.                                          */
 int gbs_tor_recursive_single_host(const double* O, int n, int g, double* out);
 int gbs_tor_single_certified_host(const double* O, int n, int g, double* out, double* bound);
+/* reference: core/host_api.cu:354-405 (gbs_tor_single_ddcertified_host): the same
+ * single-large evaluation in double-word with a rigorous bound.                  */
+int gbs_tor_single_ddcertified_host(const double* O, int n, int g, double* out, double* bound);
 
 /* ---- repeated-row loop hafnian (finite-difference sieve) ----------------------
  * reference: core/host_api.cu:409-432 (gbs_lhaf_repeated_host),

@@ -68,5 +68,15 @@ def test_tor_single_off_domain_raises(gpu):
         gpu.tor_single(1.5 * np.eye(8))
     with pytest.raises(ValueError):
         gpu.tor_single(1.5 * np.eye(8), certified=True)
-    with pytest.raises(RuntimeError, match="certified-dd"):
-        gpu.tor_single(phys_O(3), dd=True)
+    with pytest.raises(ValueError):
+        gpu.tor_single(1.5 * np.eye(8), dd=True)
+
+
+@pytest.mark.parametrize("n", [6, 12])
+def test_tor_single_dd_certified(gpu, orc, n):
+    O = phys_O(n)
+    truth = orc.tor(O, "quad").real
+    v, d = gpu.tor_single(O, dd=True)
+    assert d["tier"] == "certified-dd"
+    assert abs(v - truth) <= d["abs_error_bound"] + 1e-30
+    assert d["rel_error_bound"] < 1e-13

@@ -91,3 +91,35 @@ def test_workload_runner_small_torontonian(gpu):
     with gpu.Workspace() as ws:
         assert np.array_equal(out, ws.tor_batched(mats))
     assert np.all(aux > 0)
+
+
+@pytest.mark.parametrize("n", [3, 7, 10, 12])
+def test_tor_dd_certified_vs_binary128(gpu, orc, n):
+    # the double-double certificate: encloses the binary128 truth and is tight even
+    # where the binary64 certificate is loose
+    lib = gpu._lib.load()
+    mats = np.stack([phys_O(n), phys_O(n, 3.0)])
+    cm = np.ascontiguousarray(mats, dtype=np.complex128)
+    out = np.empty(2, np.complex128)
+    bnd = np.empty(2)
+    gpu._lib.check(lib.gbs_tor_dd_certified_host(gpu._lib.dptr(cm.view(np.float64)), n, 2,
+                                                 gpu._lib.dptr(out.view(np.float64)), gpu._lib.dptr(bnd)),
+                   "gbs_tor_dd_certified_host")
+    dd = gpu.tor_batched(mats, precision="dd")
+    for i in range(2):
+        truth = orc.tor(mats[i], "quad")
+        assert abs(out[i] - truth) <= bnd[i], (n, i, abs(out[i] - truth), bnd[i])
+        assert bnd[i] <= 1e-14 * abs(truth), (n, i, bnd[i] / abs(truth))
+        assert out[i] == dd[i]  # the certified double-double value is the dd value
+
+
+def test_certified_ladder_escalates_to_dd(gpu):
+    from gbskernels_b200 import workloads
+    O = np.stack(list(workloads.tor_click_batch(4, kmin=16, kmax=16, seed=8)))
+    v, d = gpu.tor_batched(O, precision="certified", return_diagnostics=True, rtol=1e-10)
+    dd = gpu.tor_batched(O, precision="dd")
+    for i in range(4):
+        assert d[i]["rel_error_bound"] <= 1e-10
+        if d[i]["tier"] == "certified-dd":
+            assert d[i]["escalated"] is True and v[i] == dd[i]
+    assert any(x["tier"] == "certified-dd" for x in d)  # click patterns cancel beyond binary64
