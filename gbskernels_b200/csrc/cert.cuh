@@ -142,4 +142,107 @@ __device__ __forceinline__ cball perm_lane_range_cert(const double* __restrict__
   return acc;
 }
 
+
+// ---------------------------------------------------------------------------------
+// Certified double-double Glynn walk of one lane: the value path of
+// perm_lane_range_dd (perm_tor.cuh) operation for operation, each double-word
+// complex carrying a radius that bounds the modulus of its error.  Per-operation
+// relative bounds (u = 2^-53; Joldes, Muller and Popescu, "Tight and rigorous error
+// bounds for basic building blocks of double-word arithmetic", 2017): the sum of a
+// double-word and a double 2u^2, the accurate double-word sum 3u^2/(1-4u), the
+// FMA double-word product 5u^2; charged here with slack:
+//   every double-word sum (row-sum update, acc +- p, butterfly):
+//     radius += 4u^2 (|re| + |im|) of the result
+//   complex product of two double-word complexes: per component two products and
+//     one sum, <= 9u^2 (|ac| + |bd|) (1 + O(u)); over both components
+//     (|a|+|b|)(|c|+|d|) <= 2|x||y|, so 18u^2 |x||y|, charged 21u^2 |x||y|
+// plus an absolute underflow term per operation (kUfl, 8 kUfl for a product).
+// |z| of a double-word complex is bounded by (|re.hi| + |im.hi|)(1 + 4u).
+struct ddball {
+  ddc z;
+  double r;
+};
+__device__ __forceinline__ double ddc_mag_up(const ddc& z) {
+  return ru_mul(ru_add(fabs(z.re.hi), fabs(z.im.hi)), 1.0 + 4.0 * kU);
+}
+__device__ __forceinline__ double dd_round_err(const ddc& z) {  // 4u^2 (|re| + |im|)
+  return ru_add(ru_mul(4.0 * kU * kU, ddc_mag_up(z)), kUfl);
+}
+__device__ __forceinline__ ddball ddb_mul(const ddball& x, const ddball& y) {
+  ddball o;
+  o.z = ddc_mul(x.z, y.z);
+  const double mx = ddc_mag_up(x.z), my = ddc_mag_up(y.z);
+  double r = ru_add(ru_add(ru_mul(mx, y.r), ru_mul(my, x.r)), ru_mul(x.r, y.r));
+  o.r = ru_add(r, ru_add(ru_mul(21.0 * kU * kU, ru_mul(mx, my)), 8.0 * kUfl));
+  return o;
+}
+template <int NN>
+__device__ __forceinline__ ddball tree_prod_ddb(const ddball (&v)[NN]) {
+  if constexpr (NN == 1) {
+    return v[0];
+  } else {
+    constexpr int H = NN / 2;
+    ddball lo[H], hi[NN - H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) lo[i] = v[i];
+#pragma unroll
+    for (int i = 0; i < NN - H; ++i) hi[i] = v[H + i];
+    return ddb_mul(tree_prod_ddb<H>(lo), tree_prod_ddb<NN - H>(hi));
+  }
+}
+
+template <int NN>
+__device__ __forceinline__ ddball perm_lane_range_certdd(const double* __restrict__ A2, uint64_t i0, uint64_t R) {
+  ddball rs[NN];
+  const uint64_t g0 = gray_of(i0);
+#pragma unroll
+  for (int r = 0; r < NN; ++r) {
+    ddc s = ddc{dd_make(0.0), dd_make(0.0)};
+    double rad = 0.0;
+    for (int c = 0; c < NN; ++c) {
+      cplx a = ld_c2(A2 + (r * NN + c) * 2);
+      double sg = (c > 0 && ((g0 >> (c - 1)) & 1ull)) ? -0.5 : 0.5;  // exact scaling of 2A
+      s = ddc{dd_add_d(s.re, sg * a.re), dd_add_d(s.im, sg * a.im)};
+      rad = ru_add(rad, dd_round_err(s));
+    }
+    rs[r] = ddball{s, rad};
+  }
+  bool neg = (i0 & 1ull) != 0;
+  ddball acc;
+  {
+    ddball p = tree_prod_ddb<NN>(rs);
+    acc = ddball{neg ? ddc_neg(p.z) : p.z, p.r};
+  }
+  for (uint64_t j = 1; j < R; ++j) {
+    const uint64_t i = i0 + j;
+    const int k = __ffsll((long long)j) - 1;
+    const bool minus = ((gray_of(i) >> k) & 1ull) != 0;
+    const double* col = A2 + (k + 1) * 2;
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      cplx a = ld_c2(col + r * NN * 2);  // exact 2A
+      rs[r].z.re = dd_add_d(rs[r].z.re, minus ? -a.re : a.re);
+      rs[r].z.im = dd_add_d(rs[r].z.im, minus ? -a.im : a.im);
+      rs[r].r = ru_add(rs[r].r, dd_round_err(rs[r].z));
+    }
+    neg = !neg;
+    ddball p = tree_prod_ddb<NN>(rs);
+    acc.z = neg ? ddc_sub(acc.z, p.z) : ddc_add(acc.z, p.z);
+    acc.r = ru_add(ru_add(acc.r, p.r), dd_round_err(acc.z));
+  }
+  return acc;
+}
+
+// butterfly of double-word balls (value ops those of warp_sum_ddc)
+__device__ __forceinline__ ddball warp_sum_ddb(ddball b) {
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) {
+    const ddc o = shfl_xor_ddc(b.z, m);
+    const double orr = shfl_xor_d(b.r, m);
+    b.z = ddc_add(b.z, o);
+    b.r = ru_add(ru_add(b.r, orr), dd_round_err(b.z));
+  }
+  return b;
+}
+
 }  // namespace gbsb

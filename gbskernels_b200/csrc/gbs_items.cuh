@@ -52,6 +52,12 @@ __device__ ItemResult perm_item_n(const double* A2, unsigned long long lo, unsig
     b = warp_sum_cb(b);
     r.val = ddc_from_c(b.z);
     r.aux = b.r;
+  } else if (TIER == kTierCertDD) {
+    ddball b{ddc{dd_make(0.0), dd_make(0.0)}, 0.0};
+    if (active) b = perm_lane_range_certdd<NN>(A2, i0, R);
+    b = warp_sum_ddb(b);
+    r.val = b.z;
+    r.aux = b.r;
   } else {
     double absacc = 0.0;
     cplx v = mkc(0.0, 0.0);
@@ -282,6 +288,7 @@ __device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstD
     GBSB_BR(kFnTor, kTierKappa, (tor_item<kTierKappa>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierDD, (tor_item<kTierDD>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnPerm, kTierCert, (perm_item<kTierCert>(P.mats, d, w, ws, lane)))
+    GBSB_BR(kFnPerm, kTierCertDD, (perm_item<kTierCertDD>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnHaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, false, ws, P.haf_smax, lane)))
     GBSB_BR(kFnLhaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, true, ws, P.haf_smax, lane)))
     GBSB_BR(kFnTor, kTierCert, (tor_item<kTierCert>(P.mats, d, w, ws, lane)))

@@ -170,7 +170,7 @@ static double item_cost(int fn, int dim, unsigned long long count, int tier, int
     }
     default: { double n = dim / 2.0; c = (double)count * (n + 1) * n * n * n; break; }
   }
-  return tier == kTierDD ? 20.0 * c : c;
+  return (tier == kTierDD || tier == kTierCertDD) ? 20.0 * c : c;
 }
 
 // Append one instance (already validated) to the plan.  Returns the instance index.
@@ -196,7 +196,7 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     if (terms <= 32) {
       add(0, terms);
     } else {
-      const int rcap = tier == kTierDD ? 6 : 10;
+      const int rcap = (tier == kTierDD || tier == kTierCertDD) ? 6 : 10;  // the dd tiers share one split
       int rlog = std::min(n - 1 - 5, rcap);
       const int tl = tuned_split(fn, tier, dim_eval);
       if (tl >= 0) rlog = std::min(n - 1 - 5, tl);
@@ -351,8 +351,9 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
   *real_in = false;
   if (r.dim < 0) return fail(cudaErrorInvalidValue, "negative matrix dimension");
   if (r.tier < 0 || r.tier > 4) return fail(cudaErrorInvalidValue, "unsupported precision tier");
-  if (r.tier == kTierCertDD && r.fn != kFnTor)
-    return fail(cudaErrorNotSupported, "the certified double-double tier is provided for the torontonian only");
+  if (r.tier == kTierCertDD && r.fn != kFnTor && r.fn != kFnPerm)
+    return fail(cudaErrorNotSupported,
+                "the certified double-double tier is provided for the permanent and the torontonian only");
   switch (r.fn) {
     case kFnPerm:
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
@@ -463,7 +464,7 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
       groups[g].push_back(i);
     }
   } else {
-    groups.resize(5);
+    groups.resize(6);  // everything but the permanent, then the permanent per tier (0..4)
     for (int i = 0; i < B; ++i) {
       if (s->plan_trivial[i]) continue;
       groups[reqs[i].fn == kFnPerm ? 1 + reqs[i].tier : 0].push_back(i);
@@ -902,8 +903,11 @@ int gbs_perm_certified_host(const double* m, int n, int b, double* o, double* e)
 int gbs_haf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnHaf, m, N, b, o, e); }
 int gbs_lhaf_certified_host(const double* m, int N, int b, double* o, double* e) { return one_shot_cert(kFnLhaf, m, N, b, o, e); }
 int gbs_tor_certified_host(const double* m, int n, int b, double* o, double* e) { return one_shot_cert(kFnTor, m, 2 * n, b, o, e); }
-// certified double-double torontonian: double-word value (returned rounded to
-// binary64) + rigorous bound, the rung above the binary64 certificate
+// certified double-double permanent and torontonian: double-word value (returned
+// rounded to binary64) + rigorous bound, the rung above the binary64 certificate
+int gbs_perm_dd_certified_host(const double* m, int n, int b, double* o, double* e) {
+  return one_shot_cert(kFnPerm, m, n, b, o, e, kTierCertDD);
+}
 int gbs_tor_dd_certified_host(const double* m, int n, int b, double* o, double* e) {
   return one_shot_cert(kFnTor, m, 2 * n, b, o, e, kTierCertDD);
 }

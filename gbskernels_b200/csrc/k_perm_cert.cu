@@ -3,6 +3,6 @@
 #include "gbs_items.cuh"
 
 namespace gbsb {
-#define GBSB_LIST_PERM_CERT(X) X(br1(kFnPerm, kTierCert))
+#define GBSB_LIST_PERM_CERT(X) X(br1(kFnPerm, kTierCert)) X(br1(kFnPerm, kTierCertDD))
 GBSB_DEFINE_GROUP(perm_cert, GBSB_LIST_PERM_CERT)
 }  // namespace gbsb

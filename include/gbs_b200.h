@@ -58,6 +58,12 @@ int gbs_perm_certified_host(const double* mats, int n, int batch, double* out, d
 int gbs_haf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
 int gbs_lhaf_certified_host(const double* mats, int N, int batch, double* out, double* bound);
 int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, double* bound);
+/* certified double-double permanent: the double-double Glynn walk of
+ * gbs_perm_dd_host (the value equals it before the final rounding to binary64)
+ * in ball arithmetic; the rung of the certified ladder above
+ * gbs_perm_certified_host.  reference: core/host_api.cu:263-265
+ * (gbs_perm_dd_certified_host), kernels core/certified_dd.cu:124-328.            */
+int gbs_perm_dd_certified_host(const double* mats, int n, int batch, double* out, double* bound);
 /* certified double-double torontonian (real O, 24 modes batched): the value is
  * computed in double-word arithmetic (returned rounded to binary64) and the bound
  * is rigorous; the rung of the certified ladder above gbs_tor_certified_host.
