@@ -431,14 +431,49 @@ def gpu_backend_kind() -> str:
 
 
 # ------------------------------------------------------------------ sessions / ragged batches
+class _ResidentView:
+    """A typed part (aux or status) of a resident result block, on the device."""
+
+    def __init__(self, owner: "_ResidentResult", byte_offset: int, n: int, typestr: str, dtype):
+        self._owner = owner
+        self._off = byte_offset
+        self._n = n
+        self._typestr = typestr
+        self._dtype = dtype
+
+    @property
+    def __cuda_array_interface__(self):
+        base = ctypes.cast(self._owner._ptr, ctypes.c_void_p).value or 0
+        return {"shape": (self._n,), "typestr": self._typestr, "data": (base + self._off if base else 0, False),
+                "version": 3}
+
+    def numpy(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=self._dtype)
+        if self._n:
+            if not self._owner._ptr:
+                raise RuntimeError("resident result is closed")
+            base = ctypes.cast(self._owner._ptr, ctypes.c_void_p).value
+            _lib.check(_lib.load().gbs_dev_copy_to_host(ctypes.c_void_p(base + self._off),
+                                                        out.ctypes.data_as(ctypes.c_void_p), out.nbytes),
+                       "gbs_dev_copy_to_host")
+        return out
+
+    def __len__(self) -> int:
+        return self._n
+
+
 class _ResidentResult:
     """Device-resident (B,) complex128 result (gbskernels/__init__.py:856-908 contract).
     Exposes ``__cuda_array_interface__`` so ``torch.as_tensor(r, device='cuda')`` or
-    CuPy consume it without a copy; ``.numpy()`` copies to the host."""
+    CuPy consume it without a copy; ``.numpy()`` copies to the host.  The block also
+    holds, on the device, ``.aux`` (float64: the certified bound, the indicator sum
+    or kappa, by tier) and ``.status`` (int32, 0 = ok; the value is NaN otherwise)."""
 
     def __init__(self, ptr: ctypes.POINTER(ctypes.c_double), n: int):
         self._ptr = ptr
         self._n = n
+        self.aux = _ResidentView(self, 16 * n, n, "<f8", np.float64)
+        self.status = _ResidentView(self, 24 * n, n, "<i4", np.int32)
 
     @property
     def __cuda_array_interface__(self):
@@ -448,6 +483,8 @@ class _ResidentResult:
     def numpy(self) -> np.ndarray:
         out = np.empty(self._n, dtype=np.complex128)
         if self._n:
+            if not self._ptr:
+                raise RuntimeError("resident result is closed")
             _lib.check(_lib.load().gbs_dev_to_host(self._ptr, _lib.dptr(out.view(np.float64)), self._n),
                        "gbs_dev_to_host")
         return out
@@ -618,23 +655,56 @@ class Workspace:
         return self._resident("tor", matrices, precision)
 
     def _resident(self, func: str, matrices, precision: str):
+        """Uniform batch, result left on the device in request order (every tier:
+        fp64, dd, auto -- aux = kappa --, certified -- aux = the bound)."""
         self._require()
-        if precision != "fp64":
-            raise NotImplementedError("device-resident output is fp64 only; use precision='fp64'")
+        if precision == "ref":
+            raise NotImplementedError("'ref' is the mpmath ground truth -- CPU only (backend='cpu').")
+        if precision not in ("fp64", "dd", "auto", "certified"):
+            raise ValueError(f"unknown precision {precision!r}; expected one of {PRECISIONS}")
         try:
             stack = np.ascontiguousarray(np.asarray(matrices, dtype=np.complex128))
             uniform = stack.ndim == 3
         except (ValueError, TypeError):
             uniform = False
         if not uniform:
-            raise ValueError("device-resident output needs a uniform (B, d, d) batch")
-        stack = _prepare(func, stack, precision)
+            raise ValueError("device-resident output of a ragged batch: use Workspace.evaluate_resident")
+        stack = _prepare(func, stack, "dd" if precision == "dd" else "fp64")
+        if precision == "certified":
+            _check_certified_input(stack)
+            if _is_complex_tor(func, stack):
+                raise NotImplementedError("certified torontonian is real-domain only")
+        if precision == "auto" and _is_complex_tor(func, stack):
+            raise NotImplementedError("auto torontonian of a complex O: the double-double rerun is "
+                                      "real-domain only; use precision='fp64'")
         B, d = stack.shape[0], stack.shape[1]
+        tier = {"fp64": 0, "dd": 1, "certified": 3, "auto": -1}[precision]
         ptr = ctypes.POINTER(ctypes.c_double)()
-        rc = _lib.load().gbs_session_evaluate_resident(self._session, _FN[func], 0,
-                                                       _lib.dptr(stack.view(np.float64)), d, B,
-                                                       ctypes.byref(ptr))
-        _lib.check(rc, "gbs_session_evaluate_resident")
+        rc = _lib.load().gbs_session_evaluate_resident_tier(self._session, _FN[func], tier,
+                                                            _lib.dptr(stack.view(np.float64)), d, B,
+                                                            ctypes.byref(ptr))
+        _lib.check(rc, "gbs_session_evaluate_resident_tier")
+        return _ResidentResult(ptr, B)
+
+    def evaluate_resident(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str] | None = None):
+        """Ragged, mixed-function, mixed-tier batch with the results left on the device
+        in request order (scattered there; aux and status alongside)."""
+        self._require()
+        B = len(mats)
+        precisions = precisions or ["fp64"] * B
+        if not (len(funcs) == B == len(precisions)):
+            raise ValueError("funcs, mats and precisions must have the same length")
+        if B == 0:
+            return _ResidentResult(ctypes.POINTER(ctypes.c_double)(), 0)
+        mats = _as_square_list(mats)
+        buf, dims, offs = _pack(mats)
+        fns = np.array([_FN[f] for f in funcs], dtype=np.int32)
+        tiers = np.array([_TIER[p] for p in precisions], dtype=np.int32)
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        rc = _lib.load().gbs_queue_evaluate_resident(
+            self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims), _lib.llptr(offs),
+            _lib.dptr(buf.view(np.float64)), 0 if self._persistent else 1, ctypes.byref(ptr))
+        _lib.check(rc, "gbs_queue_evaluate_resident")
         return _ResidentResult(ptr, B)
 
 

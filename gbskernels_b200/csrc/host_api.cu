@@ -118,6 +118,22 @@ struct GatherDesc {
   int d, de, M, use_gamma;
 };
 cudaError_t launch_gather(const GatherDesc* descs, int n, const int* idx, double* mats, cudaStream_t st);
+// Scatter of a plan's results to request order on the device (k_gather.cu).
+struct ScatterArgs {
+  const double* out;
+  const double* aux;
+  const int* st;
+  const int* map;
+  int ni;
+  const int* tidx;
+  const double* tval;
+  int ntriv;
+  double* dval;
+  double* daux;
+  int* dst;
+  int write_aux;
+};
+cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t st);
 
 struct Plan {
   std::vector<InstDesc> insts;
@@ -281,6 +297,8 @@ struct gbs_session {
   gbsb::PinBuf pin_in, pin_meta, pin_out;
   gbsb::DevBuf gather;
   gbsb::PinBuf pin_gather;
+  gbsb::DevBuf rmap;       // instance -> request map and trivial values of a resident read
+  gbsb::PinBuf pin_rmap;
   std::vector<gbsb::GatherDesc> gdesc;
   std::vector<int> gidx;
   size_t reallocs = 0;
@@ -301,6 +319,7 @@ struct gbs_session {
   int plan_B = 0;
   std::vector<char> plan_trivial;
   std::vector<gbsb::cplx> plan_tval;
+  std::vector<int> plan_tier;  // tier of each request
   size_t plan_ninst = 0;
   bool plan_ready = false;
   // CUDA graph of the prepared plan's launch sequence (queue resets + one launch per
@@ -437,6 +456,8 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
   s->plan_B = B;
   s->plan_trivial.assign(B, 0);
   s->plan_tval.assign(B, mkc(0, 0));
+  s->plan_tier.assign(B, 0);
+  for (int i = 0; i < B; ++i) s->plan_tier[i] = reqs[i].tier;
   s->plan_ninst = 0;
   if (B == 0) { s->plan_ready = true; return 0; }
   std::vector<int> dim_eval(B, 0);
@@ -601,10 +622,20 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
     L.ws_doubles = P.ws_doubles;
     L.haf_smax = P.haf_smax;
     G.br = cover(P.need);
-    // one-warp blocks when each warp needs a large shared workspace (the hafnian
-    // families) so the SM packs as many warps as shared memory allows
+    // with a large shared workspace per warp (the hafnian families) the block size
+    // that packs the most resident warps per SM (1, 2 or 4 warps: each block also
+    // reserves shared memory of its own, so small blocks can lose a warp)
     const size_t smem_per_warp = (size_t)P.ws_doubles * sizeof(double);
-    int warps = smem_per_warp >= 8192 ? 1 : opt.warps;
+    int warps = opt.warps;
+    if (smem_per_warp >= 8192) {
+      int best = 0;
+      for (int w = 1; w <= 4; w <<= 1) {
+        if ((size_t)w * smem_per_warp > 200 * 1024) break;
+        const int resident = occ_any(G.br, L, w) * w;
+        if (resident > best) { best = resident; warps = w; }
+      }
+      if (best == 0) warps = 1;
+    }
     if (opt.per_size && !P.insts.empty()) {  // a per-size bucket: the tuned block size, if any
       const int tw = tuned_warps(ft_fn(P.insts[0].ft), ft_tier(P.insts[0].ft), P.insts[0].dim);
       if (tw > 0) warps = tw;
@@ -720,10 +751,68 @@ static void plan_collect(gbs_session* s, double* out, double* aux, int* st) {
     const cplx t = s->plan_tval[i];
     out[2 * i] = t.re;
     out[2 * i + 1] = t.im;
-    if (aux) aux[i] = std::hypot(t.re, t.im);
+    // exact values: bound 0 for the certified tiers, |value| as the indicator sum
+    if (aux) aux[i] = tier_certified(s->plan_tier[i]) ? 0.0 : std::hypot(t.re, t.im);
     if (st) st[i] = kStOk;
   }
 }
+
+// Device-resident read: scatter the plan's results into a device block laid out as
+// [B complex values][B doubles aux][B int32 status] (request order), on `stream`.
+// `remap` (optional) sends request i of this plan to index remap[i] of the block;
+// write_aux = false keeps the block's aux entries.
+static int plan_scatter(gbs_session* s, cudaStream_t stream, double* block, int B_block,
+                        const std::vector<int>* remap, bool write_aux) {
+  if (!stream) stream = s->stream;
+  const int ni = (int)s->plan_ninst;
+  std::vector<int> tidx;
+  std::vector<double> tval;
+  for (int i = 0; i < s->plan_B; ++i) {
+    if (!s->plan_trivial[i]) continue;
+    const cplx t = s->plan_tval[i];
+    tidx.push_back(remap ? (*remap)[i] : i);
+    tval.push_back(t.re);
+    tval.push_back(t.im);
+    tval.push_back(tier_certified(s->plan_tier[i]) ? 0.0 : std::hypot(t.re, t.im));
+  }
+  const int nt = (int)tidx.size();
+  if (ni + nt == 0) return 0;
+  const size_t ints = ((size_t)ni + nt + 1) & ~(size_t)1;  // 8-byte boundary before the doubles
+  const size_t bytes = ints * sizeof(int) + tval.size() * sizeof(double);
+  cudaError_t e = cudaStreamSynchronize(stream);  // the pinned staging buffer is reused
+  if (e == cudaSuccess) e = grow_pin(s->pin_rmap, bytes);
+  if (e == cudaSuccess) e = grow_dev(s->rmap, bytes, &s->reallocs);
+  if (e != cudaSuccess) return fail(e, "staging the resident result map");
+  int* hm = (int*)s->pin_rmap.p;
+  for (const auto& G : s->groups)
+    for (int k = 0; k < G.ni; ++k) {
+      const int i = G.req[k];
+      hm[G.out_off + k] = remap ? (*remap)[i] : i;
+    }
+  for (int t = 0; t < nt; ++t) hm[ni + t] = tidx[t];
+  double* hv = (double*)(hm + ints);
+  for (size_t t = 0; t < tval.size(); ++t) hv[t] = tval[t];
+  e = cudaMemcpyAsync(s->rmap.p, s->pin_rmap.p, bytes, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return fail(e, "uploading the resident result map");
+  ScatterArgs a{};
+  a.out = (const double*)s->out.p;
+  a.aux = (const double*)s->aux.p;
+  a.st = (const int*)s->st.p;
+  a.map = (const int*)s->rmap.p;
+  a.ni = ni;
+  a.tidx = (const int*)s->rmap.p + ni;
+  a.tval = (const double*)((const int*)s->rmap.p + ints);
+  a.ntriv = nt;
+  a.dval = block;
+  a.daux = block + 2 * (size_t)B_block;
+  a.dst = (int*)(block + 3 * (size_t)B_block);
+  a.write_aux = write_aux ? 1 : 0;
+  e = launch_scatter(a, stream);
+  return e == cudaSuccess ? 0 : fail(e, "scattering the resident results");
+}
+
+// Bytes of a resident result block of B requests.
+static size_t resident_bytes(int B) { return (size_t)B * (3 * sizeof(double) + sizeof(int)); }
 
 // Copy the plan's results back (synchronous) and scatter them to request order.
 static int plan_read(gbs_session* s, cudaStream_t stream, double* out, double* aux, int* st) {
@@ -859,6 +948,84 @@ static int auto_batch(gbs_session* s, const std::vector<Req>& reqs, double kappa
       tier_out[idx[j]] = 1;
     }
   }
+  return 0;
+}
+
+// Device-resident evaluation of `reqs` into `block` (resident_bytes(B), request
+// order).  tier_mode >= 0: the requests' own tiers; kResidentAuto: fp64 + indicator,
+// the elements with kappa >= kappa_max rerun in double-double and scattered over
+// their fp64 values on the device; aux then holds kappa.  Only the kappa decision
+// reads back to the host (values and sums), as the host auto tier does.
+constexpr int kResidentAuto = -1;
+static int resident_run(gbs_session* s, std::vector<Req> reqs, int tier_mode, double kappa_max, double* block) {
+  const int B = (int)reqs.size();
+  if (B == 0) return 0;
+  RunOpts opt;
+  auto finish = [&]() -> int {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(e, "evaluating the batch");
+    float ms = 0.f;
+    if (!s->groups.empty()) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->last_kernel_ms = ms;
+    return 0;
+  };
+  if (tier_mode == kResidentAuto)
+    for (Req& r : reqs) r.tier = kTierKappa;
+  int rc = plan_build(s, reqs, opt);
+  if (rc == 0) rc = plan_launch(s, nullptr);
+  if (rc == 0) rc = plan_scatter(s, nullptr, block, B, nullptr, true);
+  if (rc == 0) rc = finish();
+  if (rc || tier_mode != kResidentAuto) return rc;
+  std::vector<double> val(2 * (size_t)B), absn(B);
+  std::vector<int> st(B);
+  cudaError_t e = cudaMemcpy(val.data(), block, val.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(absn.data(), block + 2 * (size_t)B, B * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(st.data(), block + 3 * (size_t)B, B * sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(e, "reading the indicator sums");
+  std::vector<Req> rerun;
+  std::vector<int> idx;
+  std::vector<double> kap(B);
+  for (int i = 0; i < B; ++i) {
+    const double mag = std::max(std::hypot(val[2 * i], val[2 * i + 1]), 1e-300);
+    kap[i] = absn[i] / mag;
+    if (st[i] == kStOk && !(kap[i] < kappa_max)) {
+      Req r = reqs[i];
+      r.tier = kTierDD;
+      rerun.push_back(r);
+      idx.push_back(i);
+    }
+  }
+  e = cudaMemcpy(block + 2 * (size_t)B, kap.data(), B * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(e, "writing kappa");
+  if (rerun.empty()) return 0;
+  rc = plan_build(s, rerun, opt);
+  if (rc == 0) rc = plan_launch(s, nullptr);
+  if (rc == 0) rc = plan_scatter(s, nullptr, block, B, &idx, false);
+  if (rc == 0) rc = finish();
+  return rc;
+}
+
+// A fresh resident block for B requests, evaluated; on failure nothing is kept.
+static int resident_alloc_run(gbs_session* s, const std::vector<Req>& reqs, int tier_mode, double** d_block) {
+  *d_block = nullptr;
+  const int B = (int)reqs.size();
+  if (B == 0) return 0;
+  for (const Req& r : reqs)
+    if (tier_certified(r.tier)) {
+      const size_t nn = 2ull * (size_t)r.dim * r.dim;
+      for (size_t k = 0; k < nn; ++k)
+        if (!std::isfinite(r.mat[k])) return fail(cudaErrorInvalidValue, "certified evaluation requires finite input");
+    }
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, resident_bytes(B));
+  if (e != cudaSuccess) return fail(e, "allocating the resident result block");
+  std::lock_guard<std::mutex> lk(s->mu);
+  const int rc = resident_run(s, reqs, tier_mode, 1e8, d);
+  if (rc) {
+    cudaFree(d);
+    return rc;
+  }
+  *d_block = d;
   return 0;
 }
 
@@ -1000,27 +1167,53 @@ int gbs_session_evaluate(gbs_session* s, int func, int prec, const double* h_mat
   return rc;
 }
 
-// Device-resident output: evaluate, then copy the (B,) complex results into a fresh
-// device buffer owned by the caller (freed by gbs_dev_free).
+// Device-resident output: evaluate, then scatter the (B,) complex results on the
+// device into a fresh buffer owned by the caller (freed by gbs_dev_free); nothing
+// of the result passes through the host.  prec: 0 fp64, 1 dd.
 int gbs_session_evaluate_resident(gbs_session* s, int func, int prec, const double* h_mats, int dim, int batch,
                                   double** d_result) {
   if (!s || !d_result) return fail(cudaErrorInvalidValue, "null argument");
   *d_result = nullptr;
   if (batch <= 0) return 0;
-  std::vector<double> h(2 * (size_t)batch);
-  std::vector<int> st(batch);
-  int rc = uniform(s, func, prec, h_mats, dim, batch, h.data(), nullptr, st.data());
-  if (rc) return rc;
-  apply_status(batch, h.data(), st.data());
-  double* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, h.size() * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
-    if (d) cudaFree(d);
-    return fail(e, "resident output");
-  }
-  *d_result = d;
-  return 0;
+  if (!h_mats) return fail(cudaErrorInvalidValue, "null buffer");
+  if (prec != 0 && prec != 1) return fail(cudaErrorInvalidValue, "prec must be 0 (fp64) or 1 (dd)");
+  std::vector<Req> reqs(batch);
+  const size_t stride = 2ull * dim * dim;
+  for (int i = 0; i < batch; ++i) reqs[i] = Req{func, prec, dim, h_mats + i * stride};
+  return resident_alloc_run(s, reqs, prec, d_result);
+}
+// Every tier, resident: a block [B complex values][B doubles aux][B int32 status].
+// tier: 0 fp64, 1 dd, 2 fp64 + sum|term| (aux), 3 certified (aux = bound),
+// 4 certified double-double (perm, tor), -1 auto (aux = kappa; kappa >= 1e8 -> dd).
+int gbs_session_evaluate_resident_tier(gbs_session* s, int func, int tier, const double* h_mats, int dim, int batch,
+                                       double** d_block) {
+  if (!s || !d_block) return fail(cudaErrorInvalidValue, "null argument");
+  *d_block = nullptr;
+  if (batch <= 0) return 0;
+  if (!h_mats) return fail(cudaErrorInvalidValue, "null buffer");
+  if (tier < -1 || tier > 4) return fail(cudaErrorInvalidValue, "unsupported precision tier");
+  std::vector<Req> reqs(batch);
+  const size_t stride = 2ull * dim * dim;
+  for (int i = 0; i < batch; ++i) reqs[i] = Req{func, tier < 0 ? kTierFp64 : tier, dim, h_mats + i * stride};
+  return resident_alloc_run(s, reqs, tier, d_block);
+}
+// Ragged / mixed batch, resident (the queue of gbs_queue_evaluate; results in
+// request order in a block as above).
+int gbs_queue_evaluate_resident(gbs_session* s, int B, const int* funcs, const int* tiers, const int* dims,
+                                const long long* offsets, const double* mats, int mode, double** d_block) {
+  if (!s || !d_block) return fail(cudaErrorInvalidValue, "null argument");
+  *d_block = nullptr;
+  if (B <= 0) return 0;
+  if (!funcs || !tiers || !dims || !offsets || !mats) return fail(cudaErrorInvalidValue, "null buffer");
+  std::vector<Req> reqs(B);
+  for (int i = 0; i < B; ++i) reqs[i] = Req{funcs[i], tiers[i], dims[i], mats + 2 * offsets[i]};
+  (void)mode;  // results are identical in either launch mode; the persistent queue is used
+  return resident_alloc_run(s, reqs, 0, d_block);
+}
+int gbs_dev_copy_to_host(const void* d, void* h, size_t bytes) {
+  if (bytes == 0) return 0;
+  if (!d || !h) return fail(cudaErrorInvalidValue, "null buffer");
+  return (int)cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost);
 }
 int gbs_dev_to_host(const double* d, double* h, int n) {
   if (n <= 0) return 0;

@@ -41,4 +41,61 @@ cudaError_t launch_gather(const GatherDesc* descs, int n, const int* idx, double
   return cudaGetLastError();
 }
 
+// Device-resident results: scatter of a plan's results from instance order (the
+// session's result arrays, grouped per launch) to request order in a caller-owned
+// device block, with no host round trip.  map[k] = destination index of instance k;
+// trivial requests (n = 0, odd hafnian) come as (index, re, im, aux).  A non-ok
+// status carries a NaN value (the work-item kernel already wrote it; the host
+// path applies the same convention).  Reference counterpart of the resident
+// output: core/host_api.cu:600-658 (gbs_session_evaluate_resident).
+struct ScatterArgs {
+  const double* out;
+  const double* aux;
+  const int* st;
+  const int* map;
+  int ni;
+  const int* tidx;
+  const double* tval;  // 3 per trivial request: re, im, aux
+  int ntriv;
+  double* dval;        // complex, request order
+  double* daux;
+  int* dst;
+  int write_aux;
+};
+
+__global__ void __launch_bounds__(256) scatter_kernel(ScatterArgs a) {
+  const int total = a.ni + a.ntriv;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    int i, st;
+    double re, im, x;
+    if (k < a.ni) {
+      i = a.map[k];
+      st = a.st[k];
+      re = a.out[2 * (size_t)k];
+      im = a.out[2 * (size_t)k + 1];
+      x = a.aux[k];
+      if (st != 0) re = im = __longlong_as_double(0x7ff8000000000000ll);
+    } else {
+      const int t = k - a.ni;
+      i = a.tidx[t];
+      st = 0;
+      re = a.tval[3 * t];
+      im = a.tval[3 * t + 1];
+      x = a.tval[3 * t + 2];
+    }
+    a.dval[2 * (size_t)i] = re;
+    a.dval[2 * (size_t)i + 1] = im;
+    if (a.write_aux) a.daux[i] = x;
+    a.dst[i] = st;
+  }
+}
+
+cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t st) {
+  const int total = a.ni + a.ntriv;
+  if (total <= 0) return cudaSuccess;
+  const int grid = (total + 255) / 256 < 1184 ? (total + 255) / 256 : 1184;
+  scatter_kernel<<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 }  // namespace gbsb

@@ -113,10 +113,30 @@ int gbs_session_close(gbs_session* s);
 size_t gbs_session_reallocs(const gbs_session* s);
 int gbs_session_evaluate(gbs_session* s, int func, int prec, const double* mats, int dim, int batch,
                          double* out);
+/* Device-resident output: the (B,) complex results are scattered in request order
+ * on the device into a fresh buffer (no host round trip of the results), owned by
+ * the caller and released with gbs_dev_free.                                     */
 int gbs_session_evaluate_resident(gbs_session* s, int func, int prec, const double* mats, int dim,
                                   int batch, double** d_result);
 int gbs_dev_to_host(const double* d_result, double* h_out, int n);
 int gbs_dev_free(double* d_result);
+/* Resident output for every tier: *d_block = [B complex values][B doubles aux]
+ * [B int32 status] in request order (status 0 ok, value NaN otherwise; released
+ * with gbs_dev_free).  tier: 0 fp64, 1 dd, 2 fp64 + sum|term| in aux, 3 certified
+ * (aux = rigorous bound), 4 certified double-double (perm, tor), -1 auto (fp64 +
+ * indicator, kappa >= 1e8 rerun in dd on the device; aux = kappa).
+ * reference counterpart: the resident path of core/host_api.cu:600-658 is fp64 /
+ * dd only (bindings/gbskernels_ext.cpp:209-228); the other tiers are this
+ * library's own.                                                                  */
+int gbs_session_evaluate_resident_tier(gbs_session* s, int func, int tier, const double* mats, int dim,
+                                       int batch, double** d_block);
+/* Ragged / mixed batch (as gbs_queue_evaluate), resident: a block as above.
+ * reference: gbskernels/__init__.py:856-908 refuses ragged resident batches (no
+ * device scatter there); this one scatters on the device.                        */
+int gbs_queue_evaluate_resident(gbs_session* s, int B, const int* funcs, const int* tiers, const int* dims,
+                                const long long* offsets, const double* mats, int mode, double** d_block);
+/* bytes from device memory (a resident block's aux / status parts) to the host */
+int gbs_dev_copy_to_host(const void* d, void* h, size_t bytes);
 
 /* ---- ragged, mixed-function, mixed-tier batches ----------------------------
  * reference: gbskernels/__init__.py:813-852 (Workspace._ragged: one launch per
