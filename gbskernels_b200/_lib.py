@@ -34,7 +34,11 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_perm_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
     "gbs_haf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
     "gbs_lhaf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "gbs_haf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "gbs_lhaf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
     "gbs_perm_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "gbs_haf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "gbs_lhaf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
     "gbs_tor_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
     "gbs_auto_host": ([ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _ip],
                       ctypes.c_int),

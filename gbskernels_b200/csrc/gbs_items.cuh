@@ -105,10 +105,21 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     const HafDDLayout L = haf_dd_layout(haf_smax);
     ddc acc = ddc{dd_make(0.0), dd_make(0.0)};
     for (unsigned long long k = 0; k < w.count; ++k) {
-      ddc t = haf_subset_term_dd(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      ddc t = haf_subset_term_dd<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane).z;
       acc = ddc_add(acc, t);
     }
     r.val = acc;
+  } else if (TIER == kTierCertDD) {
+    // the dd walk and its subset sum, as balls (the value is the dd value bit for bit)
+    const HafDDLayout L = haf_dd_layout(haf_smax, true);
+    ddball acc{ddc{dd_make(0.0), dd_make(0.0)}, 0.0};
+    for (unsigned long long k = 0; k < w.count; ++k) {
+      const ddball t = haf_subset_term_dd<true>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      acc = ddb_add(acc, t);
+    }
+    r.val = acc.z;
+    r.aux = acc.r;
+    if (!isfinite(acc.r) || !isfinite(acc.z.re.hi) || !isfinite(acc.z.im.hi)) r.st = kStUncertified;
   } else if (TIER == kTierCert) {
     // same grouping as the binary64 tiers (rings of kHafRing subsets, butterfly sum
     // per ring) so the certified value is the fp64 value bit for bit
@@ -291,6 +302,8 @@ __device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstD
     GBSB_BR(kFnPerm, kTierCertDD, (perm_item<kTierCertDD>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnHaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, false, ws, P.haf_smax, lane)))
     GBSB_BR(kFnLhaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnHaf, kTierCertDD, (haf_item<kTierCertDD>(P.mats, d, w, false, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnLhaf, kTierCertDD, (haf_item<kTierCertDD>(P.mats, d, w, true, ws, P.haf_smax, lane)))
     GBSB_BR(kFnTor, kTierCert, (tor_item<kTierCert>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierCertDD, (tor_item<kTierCertDD>(P.mats, d, w, ws, lane)))
 #undef GBSB_BR

@@ -15,7 +15,7 @@ namespace gbsb {
 
 // function codes (the reference's Session numbering, core/host_api.cu:472-480)
 enum : int { kFnPerm = 0, kFnHaf = 1, kFnLhaf = 2, kFnTor = 3 };
-// tier codes (kTierCertDD: double-double value + rigorous bound, torontonian only)
+// tier codes (kTierCertDD: double-double value + rigorous bound)
 enum : int { kTierFp64 = 0, kTierDD = 1, kTierKappa = 2, kTierCert = 3, kTierCertDD = 4 };
 
 __host__ __device__ constexpr int ft_code(int fn, int tier) { return fn * 8 + tier; }
@@ -50,7 +50,7 @@ constexpr unsigned kBrServe = kBrHafLhafFp64 | br1(kFnTor, kTierFp64) | br1(kFnH
                               br1(kFnLhaf, kTierCert) | br1(kFnTor, kTierCert);
 // haf / lhaf / tor in every tier
 constexpr unsigned kBrMixed = kBrServe | br1(kFnHaf, kTierDD) | br1(kFnLhaf, kTierDD) | br1(kFnTor, kTierDD) |
-                              br1(kFnTor, kTierCertDD);
+                              br1(kFnHaf, kTierCertDD) | br1(kFnLhaf, kTierCertDD) | br1(kFnTor, kTierCertDD);
 
 // Device buffers of one launch.
 struct ItemLaunch {

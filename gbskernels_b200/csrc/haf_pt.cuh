@@ -341,13 +341,46 @@ __device__ __forceinline__ void rows_bound(const double (&D)[MS][NT][4], const d
 }
 
 // ---------------------------------------------------------------------------
+// Bound path of the certified tiers for the compile-time tile shape: the powers of
+// |C| (Ca; the previous power kept in M) give the trace-bound sums
+// bT[k] += sum_{i,t} M_a[i][t] M_b[i^1][t^1] and the row bounds Ym[row][a] =
+// M_a |d| (upward rounded).  Dv holds d as binary64 complex (zero beyond s).
+template <int NT, int MS>
+__device__ __noinline__ void haf_bound_powers(const double* Ca, double* M, double* Ym, const double* Dv, double* bT,
+                                              int s, int cs, int ps, int n, int h, bool loop, int lane) {
+  const int ntn = (2 * s + 7) >> 3;  // column tiles in use (<= NT)
+  const int hp1 = h + 1;
+  double Dm[MS][NT][4];
+  load_acc<NT, MS>(Ca, cs, s, lane, Dm);
+  {
+    double tb = warp_sum_ru(even_bound<NT, MS>(Dm));
+    if (lane == 0 && 2 <= n) bT[2] = ru_add(bT[2], tb);
+  }
+  if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, 1, hp1, s, lane);
+  for (int a = 2; a <= h; ++a) {
+    const double* Qm = (a == 2) ? Ca : M;
+    const int qs = (a == 2) ? cs : ps;
+    power_product<NT, MS>(Qm, Ca, s, cs, qs, ntn, lane, Dm);
+    double bo = warp_sum_ru(odd_bound<NT, MS>(Dm, Qm, qs, s, lane));
+    double be = warp_sum_ru(even_bound<NT, MS>(Dm));
+    if (lane == 0) {
+      if (2 * a - 1 <= n) bT[2 * a - 1] = ru_add(bT[2 * a - 1], bo);
+      if (2 * a <= n) bT[2 * a] = ru_add(bT[2 * a], be);
+    }
+    __syncwarp();
+    store_acc<NT, MS>(M, ps, s, lane, Dm);
+    if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, a, hp1, s, lane);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Power loop of one subset for the compile-time tile shape (NT column tiles of 8
-// real columns, MS strips of 16 rows).  Accumulates the traces into acc_p[k], the
-// loop vectors into Y and (certified) the trace / row bound sums into bT / Ym.
-template <int NT, int MS, bool CERT>
+// real columns, MS strips of 16 rows).  Accumulates the traces into acc_p[k] and
+// the loop vectors into Y.
+template <int NT, int MS>
 __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, const double* Dv, double* acc_p,
-                                        const double* Ca, double* M, double* Ym, double* bT, int s, int cs, int ps,
-                                        int n, int h, bool loop, int lane) {
+                                        int s, int cs, int ps, int n, int h, bool loop, int lane) {
   const int ntn = (2 * s + 7) >> 3;  // column tiles in use (<= NT)
   const int hp1 = h + 1;
   double D[MS][NT][4];
@@ -358,13 +391,6 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
     if (lane == 0 && 2 <= n) st_c(acc_p + 4, cadd(ld_c(acc_p + 4), t));
   }
   if (loop) rows_times_d<NT, MS>(D, Dv, Y, 1, hp1, s, lane);
-  if constexpr (CERT) {
-    double Dm[MS][NT][4];
-    load_acc<NT, MS>(Ca, cs, s, lane, Dm);
-    double tb = warp_sum_ru(even_bound<NT, MS>(Dm));
-    if (lane == 0 && 2 <= n) bT[2] = ru_add(bT[2], tb);
-    if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, 1, hp1, s, lane);
-  }
   for (int a = 2; a <= h; ++a) {
     // the previous power: C itself (stride cs) for a = 2, then P (stride ps), in place
     const double* Q = (a == 2) ? Cs : P;
@@ -379,20 +405,6 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
     __syncwarp();
     store_acc<NT, MS>(P, ps, s, lane, D);
     if (loop) rows_times_d<NT, MS>(D, Dv, Y, a, hp1, s, lane);
-    if constexpr (CERT) {
-      const double* Qm = (a == 2) ? Ca : M;
-      double Dm[MS][NT][4];
-      power_product<NT, MS>(Qm, Ca, s, cs, qs, ntn, lane, Dm);
-      double bo = warp_sum_ru(odd_bound<NT, MS>(Dm, Qm, qs, s, lane));
-      double be = warp_sum_ru(even_bound<NT, MS>(Dm));
-      if (lane == 0) {
-        if (2 * a - 1 <= n) bT[2 * a - 1] = ru_add(bT[2 * a - 1], bo);
-        if (2 * a <= n) bT[2 * a] = ru_add(bT[2 * a], be);
-      }
-      __syncwarp();
-      store_acc<NT, MS>(M, ps, s, lane, Dm);
-      if (loop) rows_bound<NT, MS>(Dm, Dv, Ym, a, hp1, s, lane);
-    }
     __syncwarp();
   }
 }
@@ -484,8 +496,13 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   // strips with up to 8 (s <= 32); unused tiles are skipped at run time.  Few
   // shapes keep the instruction footprint small: every subset size runs one of
   // two code paths.
-  if (s <= 16) haf_powers<4, 1, CERT>(Cs, P, Y, Dv, acc_p, Ca, M, Ym, bT, s, cs, ps, n, h, loop, lane);
-  else haf_powers<8, 2, CERT>(Cs, P, Y, Dv, acc_p, Ca, M, Ym, bT, s, cs, ps, n, h, loop, lane);
+  if (s <= 16) haf_powers<4, 1>(Cs, P, Y, Dv, acc_p, s, cs, ps, n, h, loop, lane);
+  else haf_powers<8, 2>(Cs, P, Y, Dv, acc_p, s, cs, ps, n, h, loop, lane);
+  if constexpr (CERT) {
+    __syncwarp();
+    if (s <= 16) haf_bound_powers<4, 1>(Ca, M, Ym, Dv, bT, s, cs, ps, n, h, loop, lane);
+    else haf_bound_powers<8, 2>(Ca, M, Ym, Dv, bT, s, cs, ps, n, h, loop, lane);
+  }
   __syncwarp();
 
   if (loop) {

@@ -224,7 +224,7 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
     const int n = dim_eval / 2;
     const unsigned long long masks = 1ull << n;
     // masks per item: 2^7 (binary64 tiers) / 2^6 (double-double); smaller instances are one item
-    int per = tier == kTierDD ? std::min(n, 6) : std::min(n, 7);
+    int per = (tier == kTierDD || tier == kTierCertDD) ? std::min(n, 6) : std::min(n, 7);  // dd tiers: one split
     const int tl = tuned_split(fn, tier, dim_eval);
     if (tl >= 0) per = std::min(n, tl);
     const unsigned long long cnt = 1ull << per;
@@ -270,7 +270,7 @@ static int ws_for_plan(const Plan& P) {
     else if (fn == kFnTor && !d.real_in) w = tor_lu_ws_doubles();
     else if (fn == kFnTor && (tier == kTierDD || tier == kTierCertDD)) w = tor_d_layout(d.dim / 2, tier == kTierCertDD).total;
     else if (fn == kFnTor) w = tor_w_layout(d.dim / 2, tier == kTierCert).total;
-    else if (tier == kTierDD) w = haf_dd_layout(P.haf_smax).total;
+    else if (tier == kTierDD || tier == kTierCertDD) w = haf_dd_layout(P.haf_smax, tier == kTierCertDD).total;
     else w = haf_layout(P.haf_smax, tier == kTierCert).total;
     ws = std::max(ws, w);
   }
@@ -370,9 +370,7 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
   *real_in = false;
   if (r.dim < 0) return fail(cudaErrorInvalidValue, "negative matrix dimension");
   if (r.tier < 0 || r.tier > 4) return fail(cudaErrorInvalidValue, "unsupported precision tier");
-  if (r.tier == kTierCertDD && r.fn != kFnTor && r.fn != kFnPerm)
-    return fail(cudaErrorNotSupported,
-                "the certified double-double tier is provided for the permanent and the torontonian only");
+
   switch (r.fn) {
     case kFnPerm:
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
@@ -1074,6 +1072,12 @@ int gbs_tor_certified_host(const double* m, int n, int b, double* o, double* e) 
 // rounded to binary64) + rigorous bound, the rung above the binary64 certificate
 int gbs_perm_dd_certified_host(const double* m, int n, int b, double* o, double* e) {
   return one_shot_cert(kFnPerm, m, n, b, o, e, kTierCertDD);
+}
+int gbs_haf_dd_certified_host(const double* m, int N, int b, double* o, double* e) {
+  return one_shot_cert(kFnHaf, m, N, b, o, e, kTierCertDD);
+}
+int gbs_lhaf_dd_certified_host(const double* m, int N, int b, double* o, double* e) {
+  return one_shot_cert(kFnLhaf, m, N, b, o, e, kTierCertDD);
 }
 int gbs_tor_dd_certified_host(const double* m, int n, int b, double* o, double* e) {
   return one_shot_cert(kFnTor, m, 2 * n, b, o, e, kTierCertDD);

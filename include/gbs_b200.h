@@ -64,6 +64,14 @@ int gbs_tor_certified_host(const double* mats, int n, int batch, double* out, do
  * gbs_perm_certified_host.  reference: core/host_api.cu:263-265
  * (gbs_perm_dd_certified_host), kernels core/certified_dd.cu:124-328.            */
 int gbs_perm_dd_certified_host(const double* mats, int n, int batch, double* out, double* bound);
+/* certified double-double hafnian / loop hafnian: the double-double power trace of
+ * gbs_haf_dd_host / gbs_lhaf_dd_host (the value equals it before the rounding to
+ * binary64) with an a-priori radius from double-word operation bounds and the
+ * powers of |C|, to N = 32 (the reference stops at 16).
+ * reference: core/host_api.cu:266-268 (gbs_haf_dd_certified_host), kernel
+ * core/certified_dd.cu:216-328; the loop hafnian rung is this library's own.      */
+int gbs_haf_dd_certified_host(const double* mats, int N, int batch, double* out, double* bound);
+int gbs_lhaf_dd_certified_host(const double* mats, int N, int batch, double* out, double* bound);
 /* certified double-double torontonian (real O, 24 modes batched): the value is
  * computed in double-word arithmetic (returned rounded to binary64) and the bound
  * is rigorous; the rung of the certified ladder above gbs_tor_certified_host.
