@@ -325,8 +325,10 @@ def lhaf_repeated(A: Any, gamma: Any, reps: Any, backend: str = "gpu", certified
     non-negative counts (or one length-M pattern).  Returns the (B,) values (a scalar
     for one pattern) of the finite-difference sieve, ``prod(n_i + 1)`` terms per
     pattern, evaluated on the GPU (``libgbs_b200`` sieve kernel).  Caps: M <= 32,
-    sum(reps) <= 64, prod(n_i + 1) <= 2^40.  ``certified=True`` (the reference's
-    certified sieve) is not provided and raises RuntimeError."""
+    sum(reps) <= 64, prod(n_i + 1) <= 2^40.  ``certified=True``: values bit-identical
+    to the plain sieve plus a rigorous per-pattern bound; returns ``(values,
+    {"tier": "certified-fp64", "abs_error_bound": bounds})`` and raises
+    FloatingPointError when a pattern cannot be certified."""
     _check_backend(backend)
     A = np.ascontiguousarray(A, dtype=np.complex128)
     if A.ndim != 2 or A.shape[0] != A.shape[1]:
@@ -345,21 +347,35 @@ def lhaf_repeated(A: Any, gamma: Any, reps: Any, backend: str = "gpu", certified
     if (r < 0).any():
         raise ValueError("lhaf_repeated: reps must be non-negative")
     if certified:
-        raise RuntimeError("lhaf_repeated(certified=True) is not in this build")
+        _check_certified_input(A)
+        _check_certified_input(g)
     if M > 32:
         raise ValueError(f"lhaf_repeated: M = {M} exceeds the cap 32")
     if r.size and int(r.sum(axis=1).max()) > 64:
         raise ValueError("lhaf_repeated: sum(reps) exceeds the cap 64")
     B = r.shape[0]
     out = np.empty(B, dtype=np.complex128)
+    bounds = np.zeros(B, dtype=np.float64)
     if B:
         lib = _lib.load()
-        rc = lib.gbs_lhaf_repeated_host(_lib.dptr(A.view(np.float64)), _lib.dptr(g.view(np.float64)), M,
-                                        _lib.iptr(r), B, _lib.dptr(out.view(np.float64)))
+        if certified:
+            rc = lib.gbs_lhaf_repeated_cert_host(_lib.dptr(A.view(np.float64)), _lib.dptr(g.view(np.float64)), M,
+                                                 _lib.iptr(r), B, _lib.dptr(out.view(np.float64)),
+                                                 _lib.dptr(bounds))
+        else:
+            rc = lib.gbs_lhaf_repeated_host(_lib.dptr(A.view(np.float64)), _lib.dptr(g.view(np.float64)), M,
+                                            _lib.iptr(r), B, _lib.dptr(out.view(np.float64)))
         if rc != 0:
             msg = lib.gbs_lhaf_repeated_last_error()
             raise (ValueError if rc == 1 else RuntimeError)(
                 f"lhaf_repeated failed (code {rc}): {msg.decode() if msg else ''}")
+    if certified:
+        valid = (np.all(np.isfinite(out.real)) and np.all(np.isfinite(out.imag))
+                 and np.all(np.isfinite(bounds)) and np.all(bounds >= 0.0))
+        if not valid:
+            raise FloatingPointError("certified lhaf_repeated refused with a non-finite value or bound")
+        diag = {"tier": "certified-fp64", "abs_error_bound": float(bounds[0]) if single else bounds}
+        return (complex(out[0]) if single else out), diag
     return complex(out[0]) if single else out
 
 

@@ -71,6 +71,12 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_get_split": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip], ctypes.c_int),
     "gbs_queue_read": ([_vp, _vp, _dp, _dp, _ip], ctypes.c_int),
     "gbs_lhaf_repeated_host": ([_dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _dp], ctypes.c_int),
+    "gbs_lhaf_repeated_cert_host": ([_dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "gbs_sampler_sample": ([_dp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                            ctypes.c_ulonglong, _ip], ctypes.c_int),
+    "gbs_sampler_conditional_weights": ([_dp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int,
+                                         ctypes.c_int, _dp], ctypes.c_int),
+    "gbs_sampler_last_error": ([], ctypes.c_char_p),
     "gbs_lhaf_repeated_last_error": ([], ctypes.c_char_p),
     "gbs_probe_fp64_peak": ([_dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "gbs_probe_fp64_mma": ([ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),

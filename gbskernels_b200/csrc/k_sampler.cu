@@ -1,0 +1,282 @@
+// k_sampler.cu -- the resident sampler chain: per mode k the conditional
+// submatrices of every draw are gathered on the device from the reduced matrix A_k
+// and the draws' photon-count prefixes, their hafnians evaluated by the work-item
+// kernel (one work item per conditional, the queue planned on the device), and the
+// next photon count drawn by inverse CDF from a counter-based random stream -- no
+// host round trip between modes; only the final counts are read back.
+// Reference counterpart: core/sampler_gather.cu:20-57 (index rule), core/sampler_draw.cu
+// :15-47 (clip(Re haf, 0) / j! -> normalise -> inverse CDF), core/sampler_session.cu
+// :66-137 (the chain), sampling/sampler.py:214-244 (the host side: A_k and 1/j!).
+// The draw uses cuRAND's Philox4_32_10 stream per draw (subsequence = draw index), so
+// samples are distributionally, not bit-for-bit, equal to a host sampler's.
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "gbs_items.cuh"
+
+namespace gbsb {
+
+constexpr int kSamplerMaxN = 32;  // the hafnian path's cap (2 M cutoff <= 32)
+
+// One thread per (draw, candidate j): the index list of the host sampler,
+//   [mode i x prefix[i]] + [mode k-1 x j] + [mode i+k x prefix[i]] + [mode 2k-1 x j],
+// and the compact n x n submatrix A_k[idx, idx] at the slot of the instance; the
+// instance's descriptor and single work item (all 2^(n/2) subsets) are written too.
+__global__ void __launch_bounds__(128) sampler_gather_kernel(const double* __restrict__ Ak, int k,
+                                                             const int* __restrict__ state, int M, int d0,
+                                                             int ndraw, int cutoff, int slot, double* __restrict__ sub,
+                                                             InstDesc* __restrict__ insts, WorkItem* __restrict__ items,
+                                                             int* __restrict__ overflow) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ndraw * (cutoff + 1)) return;
+  const int d = d0 + t / (cutoff + 1), j = t % (cutoff + 1);
+  const int* pre = state + (size_t)d * M;
+  const int twok = 2 * k;
+  int idx[kSamplerMaxN];
+  int n = 0;
+  bool over = false;
+  auto push = [&](int v, int times) {
+    for (int r = 0; r < times; ++r) {
+      if (n < kSamplerMaxN) idx[n++] = v;
+      else over = true;
+    }
+  };
+  for (int i = 0; i < k - 1; ++i) push(i, pre[i]);
+  push(k - 1, j);
+  for (int i = 0; i < k - 1; ++i) push(i + k, pre[i]);
+  push(twok - 1, j);
+  if (n > slot) over = true;
+  if (over) {
+    atomicExch(overflow, 1);
+    n = 0;
+  }
+  double2* out = reinterpret_cast<double2*>(sub + (size_t)t * slot * slot * 2);
+  const double2* A = reinterpret_cast<const double2*>(Ak);
+  if (n == 0) {
+    // haf of the empty matrix is 1: evaluated as haf([[0, 1], [1, 0]]) = 1 (exact)
+    out[0] = make_double2(0.0, 0.0);
+    out[1] = make_double2(1.0, 0.0);
+    out[2] = make_double2(1.0, 0.0);
+    out[3] = make_double2(0.0, 0.0);
+    n = 2;
+  } else {
+    for (int r = 0; r < n; ++r)
+      for (int c = 0; c < n; ++c) out[r * n + c] = A[(size_t)idx[r] * twok + idx[c]];
+  }
+  InstDesc D{};
+  D.off = (long long)t * slot * slot * 2;
+  D.dim = n;
+  D.ft = ft_code(kFnHaf, kTierFp64);
+  D.item0 = t;
+  D.nitems = 1;
+  D.param = 0;
+  D.real_in = 0;
+  insts[t] = D;
+  WorkItem w{};
+  w.inst = t;
+  w.lo = 0;
+  w.count = 1ull << (n / 2);
+  items[t] = w;
+}
+
+// One thread per draw: weights clip(Re haf_j, 0) / j!, normalised, inverse CDF with
+// one uniform from the draw's stream; the count goes to state[d][k-1].
+__global__ void __launch_bounds__(128) sampler_draw_kernel(const double* __restrict__ haf, const double* __restrict__ invfac,
+                                                           int cutoff, int d0, int ndraw, unsigned long long seed, int k,
+                                                           int* __restrict__ state, int M) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ndraw) return;
+  const int d = d0 + t;
+  const double* w = haf + (size_t)t * (cutoff + 1) * 2;  // complex values, real parts used
+  double sum = 0.0;
+  for (int j = 0; j <= cutoff; ++j) sum += fmax(w[2 * j], 0.0) * invfac[j];
+  int photon = 0;
+  if (sum > 0.0) {
+    // stream of draw d, one uniform per mode: subsequence d, offset k - 1
+    curandStatePhilox4_32_10_t st;
+    curand_init(seed, (unsigned long long)d, (unsigned long long)(k - 1) * 4ull, &st);
+    const double u = curand_uniform_double(&st);
+    double c = 0.0;
+    for (int j = 0; j <= cutoff; ++j) {
+      c += (fmax(w[2 * j], 0.0) * invfac[j]) / sum;
+      if (c < u) ++photon;
+    }
+  }
+  state[(size_t)d * M + (k - 1)] = photon;
+}
+
+namespace {
+thread_local std::string t_sampler_err;
+int sampler_fail(int code, const std::string& msg) {
+  t_sampler_err = msg;
+  return code;
+}
+
+struct SamplerBufs {
+  double *Ak = nullptr, *invfac = nullptr, *sub = nullptr, *part = nullptr, *paux = nullptr, *out = nullptr,
+         *aux = nullptr;
+  int *state = nullptr, *head = nullptr, *done = nullptr, *pst = nullptr, *st = nullptr, *overflow = nullptr;
+  InstDesc* insts = nullptr;
+  WorkItem* items = nullptr;
+  ~SamplerBufs() {
+    for (void* p : {(void*)Ak, (void*)invfac, (void*)sub, (void*)part, (void*)paux, (void*)out, (void*)aux,
+                    (void*)state, (void*)head, (void*)done, (void*)pst, (void*)st, (void*)overflow, (void*)insts,
+                    (void*)items})
+      if (p) cudaFree(p);
+  }
+};
+
+// The chain over modes 1..M for draws [0, num_draws), in chunks whose conditional
+// submatrices fit the slot budget.  weights_out (optional, testing): the Re(haf)
+// of every (draw, j) at mode k_weights instead of drawing there.
+int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int M, int num_draws, int cutoff,
+                  const double* h_invfac, unsigned long long seed, int* h_out, int k_stop, const int* h_state_in,
+                  double* weights_out) {
+  if (M <= 0 || num_draws < 0 || cutoff < 0) return sampler_fail((int)cudaErrorInvalidValue, "sampler: bad sizes");
+  if (num_draws == 0) return 0;
+  if (!h_Ak || !h_off || (!h_invfac && !weights_out) || (!h_out && !weights_out))
+    return sampler_fail((int)cudaErrorInvalidValue, "sampler: null pointer");
+  std::vector<double> ones;
+  if (!h_invfac) {
+    ones.assign((size_t)cutoff + 1, 1.0);
+    h_invfac = ones.data();
+  }
+  if (2 * M * cutoff > kSamplerMaxN)
+    return sampler_fail((int)cudaErrorInvalidValue,
+                        "sampler: the worst-case conditional submatrix 2 M cutoff exceeds the hafnian cap 32");
+  for (int k = 1; k <= M; ++k)
+    if (h_off[k - 1] < 0 || (long long)h_off[k - 1] + 4ll * k * k > ak_total)
+      return sampler_fail((int)cudaErrorInvalidValue, "sampler: A_k offsets outside the buffer");
+  SamplerBufs B;
+  const int per = cutoff + 1;
+  const int slot_max = std::max(2, std::min(kSamplerMaxN, 2 * M * cutoff));
+  // draws per chunk: the slot buffer of one step stays within 1 GiB
+  const size_t slot_bytes = (size_t)per * slot_max * slot_max * 16;
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(num_draws, (size_t)(1ull << 30) / slot_bytes));
+  const int ninst = chunk * per;
+  cudaError_t e = cudaMalloc(&B.Ak, sizeof(double) * 2 * std::max<long long>(ak_total, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&B.invfac, sizeof(double) * per);
+  if (e == cudaSuccess) e = cudaMalloc(&B.sub, (size_t)ninst * slot_max * slot_max * 16);
+  if (e == cudaSuccess) e = cudaMalloc(&B.part, sizeof(double) * 4 * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.paux, sizeof(double) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.out, sizeof(double) * 2 * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.aux, sizeof(double) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.state, sizeof(int) * (size_t)num_draws * M);
+  if (e == cudaSuccess) e = cudaMalloc(&B.head, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&B.done, sizeof(int) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.pst, sizeof(int) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.st, sizeof(int) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.overflow, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&B.insts, sizeof(InstDesc) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.items, sizeof(WorkItem) * ninst);
+  if (e != cudaSuccess) return sampler_fail((int)e, "sampler: device allocation failed");
+  cudaStream_t s = nullptr;
+  e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return sampler_fail((int)e, "sampler: stream");
+  e = cudaMemcpyAsync(B.Ak, h_Ak, sizeof(double) * 2 * ak_total, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(B.invfac, h_invfac, sizeof(double) * per, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    if (h_state_in)
+      e = cudaMemcpyAsync(B.state, h_state_in, sizeof(int) * (size_t)num_draws * M, cudaMemcpyHostToDevice, s);
+    else
+      e = cudaMemsetAsync(B.state, 0, sizeof(int) * (size_t)num_draws * M, s);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(B.overflow, 0, sizeof(int), s);
+  // the hafnian launch: one-warp blocks, the grid from the occupancy of the kernel
+  constexpr unsigned BR = br1(kFnHaf, kTierFp64);
+  ItemLaunch L{};
+  L.mats = B.sub;
+  L.insts = B.insts;
+  L.items = B.items;
+  L.order = nullptr;
+  L.head = B.head;
+  L.done = B.done;
+  L.part = B.part;
+  L.paux = B.paux;
+  L.pst = B.pst;
+  L.out = B.out;
+  L.aux_out = B.aux;
+  L.st_out = B.st;
+  L.haf_smax = slot_max;
+  L.ws_doubles = (haf_layout(slot_max).total + 3) & ~3;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int bps = occ_br<BR>(L, 1);
+  if (bps <= 0) {
+    cudaStreamDestroy(s);
+    return sampler_fail((int)cudaErrorInvalidConfiguration, "sampler: hafnian kernel does not fit");
+  }
+  // sampling: modes 1..M; weights only: mode k_stop on the given prefixes
+  const int kmax = k_stop > 0 ? k_stop : M;
+  const int kfirst = weights_out ? kmax : 1;
+  for (int d0 = 0; d0 < num_draws && e == cudaSuccess; d0 += chunk) {
+    const int nd = std::min(chunk, num_draws - d0);
+    const int ni = nd * per;
+    for (int k = kfirst; k <= kmax && e == cudaSuccess; ++k) {
+      const int slot = std::max(2, std::min(kSamplerMaxN, 2 * k * cutoff));
+      sampler_gather_kernel<<<(ni + 127) / 128, 128, 0, s>>>(B.Ak + 2 * (size_t)h_off[k - 1], k, B.state, M, d0, nd,
+                                                            cutoff, slot, B.sub, B.insts, B.items, B.overflow);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemsetAsync(B.head, 0, sizeof(int), s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, sizeof(int) * ni, s);
+      if (e == cudaSuccess) {
+        L.n_items = ni;
+        e = launch_br<BR>(L, (int)std::min<long long>((long long)sms * bps, ni), 1, s);
+      }
+      if (e != cudaSuccess) break;
+      if (weights_out && k == kmax) {
+        std::vector<double> o(2 * (size_t)ni);
+        e = cudaMemcpyAsync(o.data(), B.out, sizeof(double) * 2 * ni, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        for (int t = 0; t < ni && e == cudaSuccess; ++t) weights_out[(size_t)d0 * per + t] = o[2 * (size_t)t];
+        break;
+      }
+      sampler_draw_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.out, B.invfac, cutoff, d0, nd, seed, k, B.state, M);
+      e = cudaGetLastError();
+    }
+  }
+  int over = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&over, B.overflow, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && h_out)
+    e = cudaMemcpyAsync(h_out, B.state, sizeof(int) * (size_t)num_draws * M, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return sampler_fail((int)e, std::string("sampler: ") + cudaGetErrorString(e));
+  if (over) return sampler_fail((int)cudaErrorInvalidValue, "sampler: a conditional submatrix exceeded its slot");
+  return 0;
+}
+}  // namespace
+
+}  // namespace gbsb
+
+using namespace gbsb;
+
+extern "C" {
+
+// h_Ak: the M reduced A-matrices concatenated (A_k is 2k x 2k complex row-major,
+// starting at complex element h_off[k-1]); ak_total complex elements.  h_out:
+// num_draws x M photon counts (row-major).  maxn is accepted for the reference's
+// signature; the slot of mode k is 2 k cutoff (<= 32, checked).
+int gbs_sampler_sample(const double* h_Ak, int ak_total, const int* h_off, int M, int num_draws, int cutoff,
+                       int maxn, const double* h_invfac, unsigned long long seed, int* h_out) {
+  (void)maxn;
+  return sampler_chain(h_Ak, ak_total, h_off, M, num_draws, cutoff, h_invfac, seed, h_out, 0, nullptr, nullptr);
+}
+
+// The conditional weights Re haf(A_k[idx, idx]) of mode k for given prefixes
+// (h_state: num_draws x M counts, columns < k - 1 used): num_draws x (cutoff + 1).
+int gbs_sampler_conditional_weights(const double* h_Ak, int ak_total, const int* h_off, int M, int k,
+                                    const int* h_state, int num_draws, int cutoff, double* h_w) {
+  if (k < 1 || k > M) return sampler_fail((int)cudaErrorInvalidValue, "sampler: mode index out of range");
+  if (!h_state || !h_w) return sampler_fail((int)cudaErrorInvalidValue, "sampler: null pointer");
+  return sampler_chain(h_Ak, ak_total, h_off, M, num_draws, cutoff, nullptr, 0, nullptr, k, h_state, h_w);
+}
+
+const char* gbs_sampler_last_error(void) { return t_sampler_err.c_str(); }
+
+}  // extern "C"

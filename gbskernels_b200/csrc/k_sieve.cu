@@ -24,6 +24,20 @@
 //     with the mu^2 powers alongside, normalisation folded into the coefficients);
 //   * item partials are reduced per pattern in item order by a second small kernel:
 //     the result is deterministic.
+//   * a non-symmetric base matrix enters as its symmetric part (A + A^T) / 2 (x^T A x
+//     only sees that part; the incremental update needs it); a symmetric one is
+//     unchanged bit for bit.
+//
+// Certified sieve (CERT; reference counterpart core/repeated.cu:158-340, which
+// recomputes every term from scratch): the same walk, so the value is the plain
+// sieve's bit for bit, with running radii in upward rounding (u = 2^-53, L1 norms
+// |re| + |im| >= |z|): the start state of an item by gamma bounds of its sums; every
+// Gray step adds the rounding of its updates (the scalings by +-2 are exact) to the
+// radii of (A x)_i, sigma^2 and mu; a parked term's S_N errs by at most
+// gamma_{8K+16} B(s~, m~) (Horner and power roundings, coefficient representation)
+// plus B(s~, m~) - B(|s|, |mu|) (its inputs' radii), B the polynomial with |cf_k|
+// evaluated upward at s~ = |s| + r_s, m~ = |mu| + r_mu; the signed binomial weight
+// carries gamma_{3 nd + 8}; sums add u |partial sum| per operation.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,6 +48,7 @@
 #include <string>
 #include <vector>
 
+#include "cert.cuh"
 #include "gbs_common.cuh"
 
 namespace gbsb {
@@ -53,6 +68,7 @@ struct SievePattern {
   int reps[kSieveMaxM];      // n of each digit
   int radix[kSieveMaxM];     // n + 1, the top digit floor(n / 2) + 1
   unsigned long long place[kSieveMaxM];  // product of the radices below the digit
+  double esym;               // certified: radius of sigma^2 from rounding (A + A^T) / 2 (0 if symmetric)
 };
 
 __device__ __forceinline__ cplx shfl_c(cplx v, int src) {
@@ -80,10 +96,30 @@ __device__ __forceinline__ cplx sieve_sn(cplx s, cplx mu, int N, const double* _
   return (N & 1) ? cmul(h, mu) : h;
 }
 
+// B(s, m) = sum_k |cf[k]| s^k m^{2(K-k)} (times m for odd N) for s, m >= 0, by
+// Horner in upward (UP) or downward rounding.
+template <bool UP>
+__device__ __forceinline__ double sieve_bpoly(double s, double m, int N, const double* __restrict__ cf) {
+  const int K = N >> 1;
+  auto mul = [](double a, double b) { return UP ? ru_mul(a, b) : rd_mul(a, b); };
+  auto add = [](double a, double b) { return UP ? ru_add(a, b) : rd_add(a, b); };
+  const double w = mul(m, m);
+  double h = fabs(cf[K]);
+  double wk = w;
+  for (int k = K - 1; k >= 0; --k) {
+    h = add(mul(h, s), mul(wk, fabs(cf[k])));
+    wk = mul(wk, w);
+  }
+  return (N & 1) ? mul(h, m) : h;
+}
+__device__ __forceinline__ double mag1_ru(cplx z) { return ru_add(fabs(z.re), fabs(z.im)); }
+
+template <bool CERT>
 __global__ void __launch_bounds__(128) sieve_kernel(const double* __restrict__ A, const double* __restrict__ gamma,
                                                     int M, const SievePattern* __restrict__ pats, int npat,
                                                     long long nitems, const double* __restrict__ coef,
-                                                    const double* __restrict__ binom, double* __restrict__ part) {
+                                                    const double* __restrict__ binom, double* __restrict__ part,
+                                                    double* __restrict__ part_r) {
   const int lane = threadIdx.x & 31;
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long it = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += warps) {
@@ -113,13 +149,32 @@ __global__ void __launch_bounds__(128) sieve_kernel(const double* __restrict__ A
     }
     double x = act ? (double)(ni - 2 * g) : 0.0;
     cplx ax = mkc(0.0, 0.0);
+    double max_ = 0.0;  // certified: sum_d |A[i][d]| |x_d|
     for (int d = 0; d < nd; ++d) {
       const int md = __shfl_sync(0xffffffffu, mi, d);
       const double xd = __shfl_sync(0xffffffffu, x, d);
-      if (act) ax = cadd(ax, cscale(ld_c(A + 2 * ((size_t)mi * M + md)), xd));
+      if (act) {
+        const cplx a = ld_c(A + 2 * ((size_t)mi * M + md));
+        ax = cadd(ax, cscale(a, xd));
+        if constexpr (CERT) max_ = ru_add(max_, ru_mul(mag1_ru(a), fabs(xd)));
+      }
     }
     cplx sig2 = warp_sum_c(cscale(ax, x));
     cplx mu = warp_sum_c(act ? cscale(ld_c(gamma + 2 * mi), x) : mkc(0.0, 0.0));
+    // certified radii (L1) of (A x)_i, sigma^2 and mu at the item start
+    double rax = 0.0, rs = 0.0, rm = 0.0;
+    if constexpr (CERT) {
+      const double g6 = gamma_ru(6.0, kU);
+      if (act) rax = ru_add(ru_mul(gamma_ru((double)nd, kU), max_), (double)nd * kUfl);
+      rs = warp_sum_ru(act ? ru_add(ru_mul(g6, ru_mul(fabs(x), mag1_ru(ax))), ru_mul(fabs(x), rax)) : 0.0);
+      rs = ru_add(rs, 64.0 * kUfl);
+      rm = warp_sum_ru(act ? ru_mul(g6, ru_mul(fabs(x), mag1_ru(ld_c(gamma + 2 * mi)))) : 0.0);
+      rm = ru_add(rm, 64.0 * kUfl);
+    }
+    const double esym = CERT ? P.esym : 0.0;
+    const int K = N >> 1;
+    const double ghorn = CERT ? gamma_ru(8.0 * K + 16.0, kU) : 0.0;
+    const double crel = CERT ? gamma_ru(3.0 * nd + 8.0, kU) : 0.0;
     double cd = act ? binom[ni * (kSieveMaxN + 1) + g] : 1.0;
     double c0 = __shfl_sync(0xffffffffu, cd, 0);
     double crest = warp_prod_d(lane == 0 ? 1.0 : cd);
@@ -129,7 +184,9 @@ __global__ void __launch_bounds__(128) sieve_kernel(const double* __restrict__ A
     // ---- walk
     cplx ps = mkc(0.0, 0.0), pm = mkc(0.0, 0.0);  // this lane's parked term
     double pc = 0.0;
+    double prs = 0.0, prm = 0.0;  // certified: the parked radii
     cplx acc = mkc(0.0, 0.0);
+    double racc = 0.0;            // certified: radius of this lane's acc
     for (unsigned long long t = t0; t < t1; ++t) {
       const int slot = (int)((t - t0) & 31ull);
       const double wgt = (2 * gtop < ntop) ? 2.0 : 1.0;
@@ -137,9 +194,27 @@ __global__ void __launch_bounds__(128) sieve_kernel(const double* __restrict__ A
         ps = sig2;
         pm = mu;
         pc = (vpar ? -wgt : wgt) * c0 * crest;
+        if constexpr (CERT) {
+          prs = ru_add(rs, esym);
+          prm = rm;
+        }
       }
       if (slot == 31 || t + 1 == t1) {
-        if (lane <= slot) acc = cadd(acc, cscale(sieve_sn(ps, pm, N, cf), pc));
+        if (lane <= slot) {
+          const cplx sn = sieve_sn(ps, pm, N, cf);
+          const cplx term = cscale(sn, pc);
+          acc = cadd(acc, term);
+          if constexpr (CERT) {
+            const double sa = mag1_ru(ps), ma = mag1_ru(pm);
+            const double bup = sieve_bpoly<true>(ru_add(sa, prs), ru_add(ma, prm), N, cf);
+            const double bdn = sieve_bpoly<false>(sa, ma, N, cf);
+            double esn = ru_add(ru_mul(ghorn, bup), ru_add(bup, -bdn));
+            esn = ru_add(esn, (double)(4 * K + 8) * kUfl);
+            double et = ru_mul(fabs(pc), esn);
+            et = ru_add(et, ru_mul(ru_add(crel, kU), ru_mul(fabs(pc), mag1_ru(sn))));
+            racc = ru_add(ru_add(racc, et), ru_add(ru_mul(kU, mag1_ru(acc)), 2.0 * kUfl));
+          }
+        }
       }
       if (t + 1 == t1) break;
       // one reflected Gray step: digit j moves by dir
@@ -159,9 +234,20 @@ __global__ void __launch_bounds__(128) sieve_kernel(const double* __restrict__ A
       const int mj = __shfl_sync(0xffffffffu, mi, j);
       const cplx axj = shfl_c(ax, j);
       const cplx ajj = ld_c(A + 2 * ((size_t)mj * M + mj));
-      sig2 = cadd(sig2, cscale(cadd(cscale(axj, 2.0), cscale(ajj, dlt)), dlt));
+      const cplx inner = cadd(cscale(axj, 2.0), cscale(ajj, dlt));
+      sig2 = cadd(sig2, cscale(inner, dlt));
       mu = cadd(mu, cscale(ld_c(gamma + 2 * mj), dlt));
-      if (act) ax = cadd(ax, cscale(ld_c(A + 2 * ((size_t)mj * M + mi)), dlt));
+      if constexpr (CERT) {
+        // the scalings by 2 and +-2 are exact; one rounding per complex sum
+        const double raxj = __shfl_sync(0xffffffffu, rax, j);
+        rs = ru_add(rs, ru_mul(2.0, ru_add(ru_mul(2.0, raxj), ru_add(ru_mul(kU, mag1_ru(inner)), kUfl))));
+        rs = ru_add(rs, ru_add(ru_mul(kU, mag1_ru(sig2)), kUfl));
+        rm = ru_add(rm, ru_add(ru_mul(kU, mag1_ru(mu)), kUfl));
+      }
+      if (act) {
+        ax = cadd(ax, cscale(ld_c(A + 2 * ((size_t)mj * M + mi)), dlt));
+        if constexpr (CERT) rax = ru_add(rax, ru_add(ru_mul(kU, mag1_ru(ax)), kUfl));
+      }
       vpar ^= 1;
       if (j == 0) {
         c0 = __shfl_sync(0xffffffffu, cd, 0);
@@ -170,18 +256,24 @@ __global__ void __launch_bounds__(128) sieve_kernel(const double* __restrict__ A
         if (j == nd - 1) gtop = __shfl_sync(0xffffffffu, g, nd - 1);
       }
     }
+    double rbut = 0.0;
+    if constexpr (CERT) rbut = ru_add(warp_sum_ru(racc), ru_mul(gamma_ru(5.0, kU), warp_sum_ru(mag1_ru(acc))));
     acc = warp_sum_c(acc);
     if (lane == 0) {
       part[2 * it] = acc.re;
       part[2 * it + 1] = acc.im;
+      if constexpr (CERT) part_r[it] = ru_add(rbut, 32.0 * kUfl);
     }
   }
 }
 
 // One warp per pattern: the item partials in item order (lane-strided, then a fixed
 // butterfly); empty patterns give 1.
+template <bool CERT>
 __global__ void __launch_bounds__(128) sieve_reduce_kernel(const SievePattern* __restrict__ pats, int npat,
-                                                           const double* __restrict__ part, double* __restrict__ out) {
+                                                           const double* __restrict__ part,
+                                                           const double* __restrict__ part_r, double* __restrict__ out,
+                                                           double* __restrict__ out_r) {
   const int lane = threadIdx.x & 31;
   const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (p >= npat) return;
@@ -190,16 +282,31 @@ __global__ void __launch_bounds__(128) sieve_reduce_kernel(const SievePattern* _
     if (lane == 0) {
       out[2 * p] = 1.0;
       out[2 * p + 1] = 0.0;
+      if constexpr (CERT) out_r[p] = 0.0;
     }
     return;
   }
   const long long nit = (long long)((P.terms + P.item_len - 1) / P.item_len);
   cplx s = mkc(0.0, 0.0);
-  for (long long k = lane; k < nit; k += 32) s = cadd(s, ld_c(part + 2 * (P.item0 + k)));
+  double r = 0.0, mg = 0.0;
+  for (long long k = lane; k < nit; k += 32) {
+    const cplx v = ld_c(part + 2 * (P.item0 + k));
+    s = cadd(s, v);
+    if constexpr (CERT) {
+      r = ru_add(r, part_r[P.item0 + k]);
+      mg = ru_add(mg, mag1_ru(v));
+    }
+  }
+  if constexpr (CERT) {
+    // lane sums of ceil(nit / 32) partials, then the butterfly: gamma_{n/32 + 5}
+    const double gs = gamma_ru((double)((nit + 31) / 32 + 5), kU);
+    r = ru_add(warp_sum_ru(r), ru_mul(gs, warp_sum_ru(mg)));
+  }
   s = warp_sum_c(s);
   if (lane == 0) {
     out[2 * p] = s.re;
     out[2 * p + 1] = s.im;
+    if constexpr (CERT) out_r[p] = ru_add(r, 32.0 * kUfl);
   }
 }
 
@@ -246,17 +353,36 @@ const SieveTables& tables() {
 
 using namespace gbsb;
 
-extern "C" {
-
-// Loop hafnians of the M x M base matrix A (complex, row-major) repeated by each
-// row of `reps` (batch x M non-negative counts), loop weights gamma (M complex, NULL =
-// zeros: ordinary hafnians of the expansions).  Caps as the reference: M <= 32,
-// N = sum(reps row) <= 64, prod(n_i + 1) <= 2^40.
-int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out) {
+namespace {
+// Plain (bound == nullptr) or certified evaluation of a batch of patterns.
+int sieve_run(const double* A_in, const double* gamma, int M, const int* reps, int batch, double* out,
+              double* bound) {
+  const bool cert = bound != nullptr;
   if (batch < 0 || M < 0) return sieve_fail((int)cudaErrorInvalidValue, "lhaf_repeated: negative size");
   if (batch == 0) return 0;
-  if (!A || !reps || !out) return sieve_fail((int)cudaErrorInvalidValue, "lhaf_repeated: null pointer");
+  if (!A_in || !reps || !out) return sieve_fail((int)cudaErrorInvalidValue, "lhaf_repeated: null pointer");
   if (M > kSieveMaxM) return sieve_fail((int)cudaErrorInvalidValue, "lhaf_repeated: M above the cap 32");
+  if (cert) {
+    for (size_t k = 0; k < 2ull * M * M; ++k)
+      if (!std::isfinite(A_in[k]))
+        return sieve_fail((int)cudaErrorInvalidValue, "certified lhaf_repeated requires finite input");
+    if (gamma)
+      for (size_t k = 0; k < 2ull * M; ++k)
+        if (!std::isfinite(gamma[k]))
+          return sieve_fail((int)cudaErrorInvalidValue, "certified lhaf_repeated requires finite input");
+  }
+  // x^T A x sees only the symmetric part: (A + A^T) / 2, bit-identical to A when
+  // A is symmetric (a + a = 2a and the halving are exact)
+  std::vector<double> As(2 * (size_t)std::max(M * M, 1), 0.0);
+  bool sym = true;
+  for (int i = 0; i < M; ++i)
+    for (int j = 0; j < M; ++j)
+      for (int c = 0; c < 2; ++c) {
+        const double a = A_in[2 * ((size_t)i * M + j) + c], b = A_in[2 * ((size_t)j * M + i) + c];
+        if (a != b) sym = false;
+        As[2 * ((size_t)i * M + j) + c] = (a + b) * 0.5;
+      }
+  const double* A = As.data();
   const SieveTables& T = tables();
   std::vector<SievePattern> pats((size_t)batch);
   long long items = 0;
@@ -294,9 +420,21 @@ int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const in
     items += (long long)((P.terms + len - 1) / len);
     if (items > kSieveMaxItems)
       return sieve_fail((int)cudaErrorInvalidValue, "lhaf_repeated: batch too large for one call (split it)");
+    // certified, non-symmetric A: |x^T (A^s - (A + A^T)/2) x| <= u sum n_i n_j |A^s_ij|
+    // (one rounding per entry of the symmetric part), charged as 2.25 u
+    P.esym = 0.0;
+    if (cert && !sym) {
+      long double e = 0.0L;
+      for (int i = 0; i < M; ++i)
+        for (int j = 0; j < M; ++j)
+          e += (long double)n[i] * n[j] *
+               (std::fabs(As[2 * ((size_t)i * M + j)]) + std::fabs(As[2 * ((size_t)i * M + j) + 1]));
+      P.esym = std::nextafter((double)(e * 2.5e-16L), INFINITY);
+    }
     pats[p] = P;
   }
   double *dA = nullptr, *dg = nullptr, *dcoef = nullptr, *dbin = nullptr, *dpart = nullptr, *dout = nullptr;
+  double *dpart_r = nullptr, *dout_r = nullptr;
   SievePattern* dpats = nullptr;
   std::vector<double> g0;
   if (!gamma) {
@@ -310,6 +448,8 @@ int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const in
   if (e == cudaSuccess) e = cudaMalloc(&dpart, sizeof(double) * 2 * std::max(items, 1ll));
   if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * 2 * batch);
   if (e == cudaSuccess) e = cudaMalloc(&dpats, sizeof(SievePattern) * batch);
+  if (e == cudaSuccess && cert) e = cudaMalloc(&dpart_r, sizeof(double) * std::max(items, 1ll));
+  if (e == cudaSuccess && cert) e = cudaMalloc(&dout_r, sizeof(double) * batch);
   if (e == cudaSuccess && M > 0) e = cudaMemcpy(dA, A, sizeof(double) * 2 * M * M, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && M > 0) e = cudaMemcpy(dg, gamma, sizeof(double) * 2 * M, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dcoef, T.coef.data(), sizeof(double) * T.coef.size(), cudaMemcpyHostToDevice);
@@ -321,18 +461,49 @@ int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const in
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long want = (items + 3) / 4;
     const int grid = (int)std::max(1ll, std::min<long long>(want, (long long)sms * 16));
-    sieve_kernel<<<grid, 128>>>(dA, dg, M, dpats, batch, items, dcoef, dbin, dpart);
+    if (cert) sieve_kernel<true><<<grid, 128>>>(dA, dg, M, dpats, batch, items, dcoef, dbin, dpart, dpart_r);
+    else sieve_kernel<false><<<grid, 128>>>(dA, dg, M, dpats, batch, items, dcoef, dbin, dpart, nullptr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
-    sieve_reduce_kernel<<<(batch + 3) / 4, 128>>>(dpats, batch, dpart, dout);
+    if (cert) sieve_reduce_kernel<true><<<(batch + 3) / 4, 128>>>(dpats, batch, dpart, dpart_r, dout, dout_r);
+    else sieve_reduce_kernel<false><<<(batch + 3) / 4, 128>>>(dpats, batch, dpart, nullptr, dout, nullptr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost);
-  for (void* p : {(void*)dA, (void*)dg, (void*)dcoef, (void*)dbin, (void*)dpart, (void*)dout, (void*)dpats})
+  if (e == cudaSuccess && cert) e = cudaMemcpy(bound, dout_r, sizeof(double) * batch, cudaMemcpyDeviceToHost);
+  for (void* p : {(void*)dA, (void*)dg, (void*)dcoef, (void*)dbin, (void*)dpart, (void*)dout, (void*)dpats,
+                  (void*)dpart_r, (void*)dout_r})
     if (p) cudaFree(p);
   if (e != cudaSuccess) return sieve_fail((int)e, std::string("lhaf_repeated: ") + cudaGetErrorString(e));
+  if (cert)
+    for (int p = 0; p < batch; ++p) {
+      // the value is returned in binary64 as computed; a non-finite value or bound
+      // is a refusal (NaN, +inf)
+      if (!std::isfinite(out[2 * p]) || !std::isfinite(out[2 * p + 1]) || !std::isfinite(bound[p])) {
+        out[2 * p] = out[2 * p + 1] = NAN;
+        bound[p] = INFINITY;
+      }
+    }
   return 0;
+}
+}  // namespace
+
+extern "C" {
+
+// Loop hafnians of the M x M base matrix A (complex, row-major) repeated by each
+// row of `reps` (batch x M non-negative counts), loop weights gamma (M complex, NULL =
+// zeros: ordinary hafnians of the expansions).  Caps as the reference: M <= 32,
+// N = sum(reps row) <= 64, prod(n_i + 1) <= 2^40.
+int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out) {
+  return sieve_run(A, gamma, M, reps, batch, out, nullptr);
+}
+
+// Certified: the same values bit for bit and a rigorous bound per pattern.
+int gbs_lhaf_repeated_cert_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out,
+                                double* bound) {
+  if (batch > 0 && !bound) return sieve_fail((int)cudaErrorInvalidValue, "lhaf_repeated: null bound buffer");
+  return sieve_run(A, gamma, M, reps, batch, out, bound ? bound : nullptr);
 }
 
 const char* gbs_lhaf_repeated_last_error(void) { return t_sieve_err.c_str(); }

@@ -99,10 +99,36 @@ int gbs_tor_single_ddcertified_host(const double* O, int n, int g, double* out, 
  * A: M x M complex base matrix; gamma: M complex loop weights (NULL = zeros, the
  * ordinary hafnian of the expansion); reps: batch x M non-negative counts; out:
  * batch complex values lhaf(A repeated by reps[b]).  Caps: M <= 32, N = sum(reps[b])
- * <= 64, prod(reps[b][i] + 1) <= 2^40.  The reference's certified variant
- * (gbs_lhaf_repeated_cert_host) is not provided.                                */
+ * <= 64, prod(reps[b][i] + 1) <= 2^40.  A non-symmetric A enters as its symmetric
+ * part (A + A^T)/2, the only part x^T A x sees.                                    */
 int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out);
+/* certified sieve: values bit-identical to gbs_lhaf_repeated_host and a rigorous
+ * bound per pattern (bound[b] >= |out[b] - lhaf|); non-finite input is rejected, an
+ * uncertifiable pattern returns NaN with bound +inf.
+ * reference: core/host_api.cu:434-458 (gbs_lhaf_repeated_cert_host), kernel
+ * core/repeated.cu:158-340.                                                       */
+int gbs_lhaf_repeated_cert_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out,
+                                double* bound);
 const char* gbs_lhaf_repeated_last_error(void);
+
+/* ---- resident sampler chain (on-device conditional draw) ---------------------
+ * reference: core/sampler_session.cu:106-137 (gbs_sampler_sample), kernels
+ * core/sampler_gather.cu:20-57 and core/sampler_draw.cu:15-47.
+ * h_Ak: the M reduced A-matrices (A_k: 2k x 2k complex, row-major) concatenated,
+ * A_k starting at complex element h_off[k-1]; ak_total complex elements in all.
+ * Per mode k = 1..M the conditional submatrices A_k[idx, idx] of every draw are
+ * gathered on the device, their hafnians evaluated by the work-item kernel and the
+ * count drawn by inverse CDF of clip(Re haf, 0) * h_invfac[j] (one Philox4_32_10
+ * uniform per draw and mode, subsequence = draw index); h_out: num_draws x M counts.
+ * Requires 2 M cutoff <= 32 (maxn is accepted for the reference's signature).      */
+int gbs_sampler_sample(const double* h_Ak, int ak_total, const int* h_off, int M, int num_draws, int cutoff,
+                       int maxn, const double* h_invfac, unsigned long long seed, int* h_out);
+/* the conditional weights Re haf(A_k[idx, idx]) of mode k for the prefixes in
+ * h_state (num_draws x M counts; columns < k-1 used): h_w is num_draws x (cutoff+1).
+ * No reference counterpart (a parity hook for the gather and hafnian steps).       */
+int gbs_sampler_conditional_weights(const double* h_Ak, int ak_total, const int* h_off, int M, int k,
+                                    const int* h_state, int num_draws, int cutoff, double* h_w);
+const char* gbs_sampler_last_error(void);
 
 /* ---- auto tier on the device ----------------------------------------------
  * reference: gbskernels/__init__.py:272-297 (_gpu_auto_batched) whose fp64 pass is

@@ -121,3 +121,18 @@ def test_tuned_split_table(lib):
     assert lib.gbs_get_split(1, 1, 20, _lib.iptr(s), _lib.iptr(w)) == 0 and s[0] == -1  # dd separate
     assert lib.gbs_set_split(1, 0, 20, -1, 0) == 0
     assert lib.gbs_set_split(9, 0, 20, 6, 0) != 0 and lib.gbs_set_split(1, 0, 99, 6, 0) != 0
+
+
+def test_sampler_reduced_A_host_construction():
+    # A = X (I - Q^-1): zero for the vacuum; for one squeezed mode (xxpp, hbar = 2)
+    # the two diagonal blocks are conjugate, of modulus tanh r
+    from gbskernels_b200 import sampler
+    assert np.allclose(sampler.reduced_A(np.eye(2), 1), 0.0)
+    r = 0.7
+    cov = np.diag([np.exp(-2 * r), np.exp(2 * r)])
+    A = sampler.reduced_A(cov, 1)
+    assert np.allclose(A, A.T)
+    assert abs(abs(A[0, 0]) - np.tanh(r)) < 1e-12 and abs(A[1, 1] - np.conj(A[0, 0])) < 1e-12
+    assert abs(A[0, 1]) < 1e-12
+    with pytest.raises(ValueError):
+        sampler.sample_resident(np.eye(10), 4, cutoff=4)  # 2 M cutoff = 40 > 32
