@@ -155,11 +155,11 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     double absacc = 0.0;
     int cnt = 0;
     for (unsigned long long k = 0; k < w.count; ++k) {
-      haf_subset_term_tc<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane, ring + cnt * kHafRingSlot * 2);
+      haf_subset_term_tc<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane, ring + cnt * L.slot * 2);
       if (++cnt == kHafRing || k + 1 == w.count) {
         __syncwarp();
         double ab = 0.0;
-        const cplx t = haf_ring_flush(ring, cnt, n, lane, TIER == kTierKappa ? &ab : nullptr);
+        const cplx t = haf_ring_flush(ring, L.slot, cnt, n, lane, TIER == kTierKappa ? &ab : nullptr);
         acc = cadd(acc, t);
         absacc += ab;
         cnt = 0;
@@ -390,10 +390,14 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
 
 // ------------------------------------------------------------------ launch helpers
 template <unsigned BR>
-static cudaError_t ensure_smem_br(size_t smem) {
+inline cudaError_t ensure_smem_br(size_t smem) {
   // the kernel's dynamic shared-memory limit only grows; once it is high enough no
   // attribute call is made, so a launch inside a stream capture issues none
-  // (per device: the attribute belongs to the device's context)
+  // (per device: the attribute belongs to the device's context).  The function has
+  // external linkage so that every translation unit that launches
+  // gbs_items_kernel<BR> (the linker keeps one copy of the kernel's host stub) shares
+  // ONE record: a per-unit record let one unit lower the limit below what another
+  // unit had set and still believed in force.
   constexpr int kDevs = 64;
   static std::atomic<size_t> smem_set[kDevs];
   static std::mutex mu;

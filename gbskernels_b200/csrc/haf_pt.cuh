@@ -46,17 +46,20 @@ __host__ __device__ inline int haf_p_stride(int s) { return (s % 4 == 2) ? s : s
 __host__ __device__ inline int haf_strips(int s) { return (s + 15) / 16; }
 
 // Per-warp shared-memory workspace (doubles), laid out for a launch-wide max s.
+// The 16-row strips of a subset run their power chains one after the other, so
+// the power and the loop vectors are held for one strip only.
 // Batched Newton recurrence: the traces of kHafRing consecutive subsets are parked
-// in a ring (slot: kg[1..n] and the sign), then kHafRing lanes run one recurrence
-// each.  Slot k[0] holds (sign, 0) or (0, 0) for an empty subset.
+// in a ring (slot: kg[1..n] and the sign, n <= smax / 2), then kHafRing lanes run
+// one recurrence each.  Slot k[0] holds (sign, 0) or (0, 0) for an empty subset.
 constexpr int kHafRing = 8;
-constexpr int kHafRingSlot = kHafMaxPairs + 1;  // complex entries per slot
 
 struct HafLayout {
   int smax;
+  int slot;  // complex entries per ring slot (smax / 2 + 1)
   int c_off, p_off, y_off, d_off, gi_off, acc_off, ring_off, total;  // in doubles
-  // certified tier only: |C|, the bound-path power, row bounds and trace-bound sums
-  int ca_off, m_off, ym_off, bt_off;
+  // certified tier only: |C|, the bound-path power, row bounds, trace-bound sums,
+  // the Newton coefficients
+  int ca_off, m_off, ym_off, bt_off, ev_off;
 };
 __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   HafLayout L;
@@ -65,25 +68,43 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   const int cs = haf_c_stride(smax), ps = haf_p_stride(smax);
   const int rows = 16 * haf_strips(smax);
   const int h = (smax / 2 + 1) / 2;
+  const int np1 = smax / 2 + 1;
+  L.slot = np1;
   L.c_off = 0;
-  L.p_off = L.c_off + rows * cs * 2;
-  L.y_off = L.p_off + rows * ps * 2;
-  L.d_off = L.y_off + rows * (h + 1) * 2;
-  L.gi_off = L.d_off + 32 * 2;   // 32 ints
-  L.acc_off = L.gi_off + 16;
-  L.ring_off = L.acc_off + 4 * (kHafMaxPairs + 1) * 2;
-  L.total = L.ring_off + kHafRing * kHafRingSlot * 2;
+  L.p_off = L.c_off + rows * cs * 2;       // C, every strip (zero padding rows)
+  L.y_off = L.p_off + 16 * ps * 2;         // the power of one strip
+  L.d_off = L.y_off + 16 * (h + 1) * 2;    // the loop vectors of one strip
+  L.gi_off = L.d_off + smax * 2;           // d
+  L.acc_off = L.gi_off + ((smax + 3) / 4) * 2;  // smax ints, 16-byte multiple
+  L.ring_off = L.acc_off + 2 * np1 * 2;    // acc_p, acc_v
+  L.total = L.ring_off + kHafRing * np1 * 2;
   L.total = (L.total + 1) & ~1;  // 16-byte multiple
-  L.ca_off = L.m_off = L.ym_off = L.bt_off = 0;
+  L.ca_off = L.m_off = L.ym_off = L.bt_off = L.ev_off = 0;
   if (cert) {
     L.ca_off = L.total;
     L.m_off = L.ca_off + rows * cs * 2;
     L.ym_off = L.m_off + rows * ps * 2;
     L.bt_off = L.ym_off + rows * (h + 1);
-    L.total = L.bt_off + 2 * (kHafMaxPairs + 2);
+    L.ev_off = L.bt_off + 2 * (kHafMaxPairs + 2);
+    L.total = L.ev_off + (kHafMaxPairs + 1) * 2;
     L.total = (L.total + 1) & ~1;
   }
   return L;
+}
+
+// Sum of four values over the warp, scattered: every lane gets the total of value
+// 2 ((lane >> 4) & 1) + ((lane >> 3) & 1) (6 shuffles instead of 4 x 5).
+__device__ __forceinline__ double warp_sum4_scatter(double v0, double v1, double v2, double v3, int lane) {
+  const bool b4 = (lane & 16) != 0, b3 = (lane & 8) != 0;
+  double k0 = b4 ? v2 : v0, k1 = b4 ? v3 : v1;
+  k0 += shfl_xor_d(b4 ? v0 : v2, 16);
+  k1 += shfl_xor_d(b4 ? v1 : v3, 16);
+  double k = b3 ? k1 : k0;
+  k += shfl_xor_d(b3 ? k0 : k1, 8);
+  k += shfl_xor_d(k, 4);
+  k += shfl_xor_d(k, 2);
+  k += shfl_xor_d(k, 1);
+  return k;
 }
 
 // ---------------------------------------------------------------------------
@@ -93,7 +114,7 @@ template <int NT, int MS>
 __device__ __forceinline__ void power_product(const double* __restrict__ P, const double* __restrict__ Cs, int s,
                                               int cs, int ps, int ntn, int lane, double (&D)[MS][NT][4]) {
   // P: the previous power (A operand, row stride ps complex); Cs: C (B' source, stride cs)
-  constexpr int KS2 = (MS == 1) ? 2 : 1;  // one strip: split K so eight mma chains are in flight
+  constexpr int KS2 = (MS == 1 && NT <= 4) ? 2 : 1;  // few tiles: split K so eight mma chains are in flight
   const int g = lane >> 2, t4 = lane & 3;
   double acc[KS2][MS][NT][4];
 #pragma unroll
@@ -215,19 +236,20 @@ __device__ __forceinline__ void store_acc(double* P, int ps, int s, int lane, co
 }
 
 // Lane partial of sum_{i,t} D[i][t] * D[i^1][t^1] (partner in lane ^ 5, same slot).
+// (four independent accumulators: rows g / g + 8 x even / odd tiles)
 template <int NT, int MS>
 __device__ __forceinline__ cplx even_partial(const double (&D)[MS][NT][4]) {
-  cplx acc = mkc(0.0, 0.0);
+  cplx acc[4] = {mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0)};
 #pragma unroll
   for (int ms = 0; ms < MS; ++ms)
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
       const double p0 = shfl_xor_d(D[ms][nt][0], 5), p1 = shfl_xor_d(D[ms][nt][1], 5);
       const double p2 = shfl_xor_d(D[ms][nt][2], 5), p3 = shfl_xor_d(D[ms][nt][3], 5);
-      acc = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), mkc(p0, p1), acc);
-      acc = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), mkc(p2, p3), acc);
+      acc[2 * (nt & 1)] = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), mkc(p0, p1), acc[2 * (nt & 1)]);
+      acc[2 * (nt & 1) + 1] = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), mkc(p2, p3), acc[2 * (nt & 1) + 1]);
     }
-  return acc;
+  return cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3]));
 }
 
 // Lane partial of sum_{i,t} D[i][t] * Q[i^1][t^1], Q the previous power in shared memory.
@@ -235,7 +257,7 @@ template <int NT, int MS>
 __device__ __forceinline__ cplx odd_partial(const double (&D)[MS][NT][4], const double* Q, int ps, int s,
                                             int lane) {
   const int g = lane >> 2, t4 = lane & 3;
-  cplx acc = mkc(0.0, 0.0);
+  cplx acc[4] = {mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0)};
 #pragma unroll
   for (int ms = 0; ms < MS; ++ms)
 #pragma unroll
@@ -245,11 +267,11 @@ __device__ __forceinline__ cplx odd_partial(const double (&D)[MS][NT][4], const 
         const int cp = col ^ 1;
         const cplx q0 = ld_c(Q + ((16 * ms + (g ^ 1)) * ps + cp) * 2);
         const cplx q1 = ld_c(Q + ((16 * ms + ((g + 8) ^ 1)) * ps + cp) * 2);
-        acc = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), q0, acc);
-        acc = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), q1, acc);
+        acc[2 * (nt & 1)] = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), q0, acc[2 * (nt & 1)]);
+        acc[2 * (nt & 1) + 1] = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), q1, acc[2 * (nt & 1) + 1]);
       }
     }
-  return acc;
+  return cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3]));
 }
 
 // y[row] = sum_t D[row][t] d[t] for the rows of this lane's group; lanes t4 == 0
@@ -375,37 +397,63 @@ __device__ __noinline__ void haf_bound_powers(const double* Ca, double* M, doubl
 }
 
 // ---------------------------------------------------------------------------
-// Power loop of one subset for the compile-time tile shape (NT column tiles of 8
-// real columns, MS strips of 16 rows).  Accumulates the traces into acc_p[k] and
-// the loop vectors into Y.
-template <int NT, int MS>
+// Power loop of one subset for the compile-time tile width (NT column tiles of 8
+// real columns): the 16-row strips run their chains C, C^2, ..., C^h one after the
+// other (the rows of a power evolve independently and a trace pair (i, i^1) never
+// crosses a strip), each with the strip's power in P and its loop vectors in Y.
+// Traces go to acc_p[k], the loop terms v_k = 1/2 sum_i y_a[i^1] y_b[i] to acc_v[k],
+// strip by strip in a fixed order.
+template <int NT>
 __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, const double* Dv, double* acc_p,
-                                        int s, int cs, int ps, int n, int h, bool loop, int lane) {
+                                        double* acc_v, int s, int cs, int ps, int n, int h, bool loop, int lane) {
   const int ntn = (2 * s + 7) >> 3;  // column tiles in use (<= NT)
   const int hp1 = h + 1;
-  double D[MS][NT][4];
-  // power 1 (= C, read in place with stride cs): p_2 and y_1
-  load_acc<NT, MS>(Cs, cs, s, lane, D);
-  {
-    cplx t = warp_sum_c(even_partial<NT, MS>(D));
-    if (lane == 0 && 2 <= n) st_c(acc_p + 4, cadd(ld_c(acc_p + 4), t));
-  }
-  if (loop) rows_times_d<NT, MS>(D, Dv, Y, 1, hp1, s, lane);
-  for (int a = 2; a <= h; ++a) {
-    // the previous power: C itself (stride cs) for a = 2, then P (stride ps), in place
-    const double* Q = (a == 2) ? Cs : P;
-    const int qs = (a == 2) ? cs : ps;
-    power_product<NT, MS>(Q, Cs, s, cs, qs, ntn, lane, D);
-    cplx to = warp_sum_c(odd_partial<NT, MS>(D, Q, qs, s, lane));
-    cplx te = warp_sum_c(even_partial<NT, MS>(D));
-    if (lane == 0) {
-      if (2 * a - 1 <= n) st_c(acc_p + 2 * (2 * a - 1), cadd(ld_c(acc_p + 2 * (2 * a - 1)), to));
-      if (2 * a <= n) st_c(acc_p + 2 * (2 * a), cadd(ld_c(acc_p + 2 * (2 * a)), te));
+  const int strips = haf_strips(s);
+  const int vq = (lane >> 3) & 3;          // the total this lane holds after warp_sum4_scatter
+  const bool vlead = (lane & 7) == 0;
+  for (int ms = 0; ms < strips; ++ms) {
+    const int r0 = 16 * ms;
+    const double* Cstrip = Cs + r0 * cs * 2;
+    double D[1][NT][4];
+    if (loop && lane < 16) st_c(Y + (lane * hp1) * 2, r0 + lane < s ? ld_c(Dv + (r0 + lane) * 2) : mkc(0.0, 0.0));
+    // power 1 (= the strip of C, read in place with stride cs): p_2 and y_1
+    load_acc<NT, 1>(Cstrip, cs, s, lane, D);
+    {
+      const cplx t = even_partial<NT, 1>(D);
+      const double tot = warp_sum4_scatter(t.re, t.im, 0.0, 0.0, lane);
+      if (vlead && vq < 2 && 2 <= n) acc_p[4 + vq] += tot;
     }
-    __syncwarp();
-    store_acc<NT, MS>(P, ps, s, lane, D);
-    if (loop) rows_times_d<NT, MS>(D, Dv, Y, a, hp1, s, lane);
-    __syncwarp();
+    if (loop) rows_times_d<NT, 1>(D, Dv, Y, 1, hp1, s, lane);
+    for (int a = 2; a <= h; ++a) {
+      // the previous power: the strip of C (stride cs) for a = 2, then P (stride ps), in place
+      const double* Q = (a == 2) ? Cstrip : P;
+      const int qs = (a == 2) ? cs : ps;
+      power_product<NT, 1>(Q, Cs, s, cs, qs, ntn, lane, D);
+      const cplx to = odd_partial<NT, 1>(D, Q, qs, s, lane);
+      const cplx te = even_partial<NT, 1>(D);
+      const double tot = warp_sum4_scatter(to.re, to.im, te.re, te.im, lane);
+      if (vlead) {
+        const int k = vq < 2 ? 2 * a - 1 : 2 * a;
+        if (k <= n) acc_p[2 * k + (vq & 1)] += tot;
+      }
+      __syncwarp();
+      store_acc<NT, 1>(P, ps, s, lane, D);
+      if (loop) rows_times_d<NT, 1>(D, Dv, Y, a, hp1, s, lane);
+      __syncwarp();
+    }
+    if (loop) {
+      // this strip's share of v_k (lane k - 1, rows in order)
+      __syncwarp();
+      if (lane < n) {
+        const int k = lane + 1;
+        const int aa = (k - 1) >> 1, bb = k - 1 - aa;
+        const int nr = min(16, s - r0);
+        cplx t = mkc(0.0, 0.0);
+        for (int i = 0; i < nr; ++i) t = cadd(t, cmul(ld_c(Y + ((i ^ 1) * hp1 + aa) * 2), ld_c(Y + (i * hp1 + bb) * 2)));
+        st_c(acc_v + 2 * k, cadd(ld_c(acc_v + 2 * k), cscale(t, 0.5)));
+      }
+      __syncwarp();
+    }
   }
 }
 
@@ -413,8 +461,9 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
 // Evaluate the signed power-trace term of one subset `mask` of instance A (N x N
 // complex, row-major, N = 2n even).  Returns the same ball in every lane (radius 0
 // unless CERT).  `loop` selects the loop hafnian; `ws` is this warp's workspace.
-// With `slot` (binary64 tiers): park kg[1..n] and the sign in the ring slot instead
-// of running the Newton recurrence (haf_ring_flush runs it for a whole ring).
+// Binary64 tiers (CERT false): kg[1..n] and the sign are parked in the ring slot
+// `slot` (required) instead of running the Newton recurrence (haf_ring_flush runs
+// it for a whole ring); the certified tier runs it in ball arithmetic here.
 template <bool CERT>
 static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, int n, uint32_t mask,
                                            bool loop, double* ws, const HafLayout& Lw, int lane,
@@ -429,14 +478,13 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   const int h = (n + 1) / 2, hp1 = h + 1;
   const int rows = 16 * haf_strips(s);
   double* Cs = ws + Lw.c_off;
-  double* P = ws + Lw.p_off;
-  double* Y = ws + Lw.y_off;        // [rows][h+1] complex
+  double* P = ws + Lw.p_off;        // one strip of the power
+  double* Y = ws + Lw.y_off;        // one strip of loop vectors: [16][h+1] complex
   double* Dv = ws + Lw.d_off;       // d[0..s)
   int* gi = reinterpret_cast<int*>(ws + Lw.gi_off);
   double* acc_p = ws + Lw.acc_off;  // p[0..n]
-  double* acc_v = acc_p + (kHafMaxPairs + 1) * 2;
-  double* kg = acc_v + (kHafMaxPairs + 1) * 2;
-  double* ev = kg + (kHafMaxPairs + 1) * 2;
+  double* acc_v = acc_p + Lw.slot * 2;
+  double* ev = ws + Lw.ev_off;      // certified tier: the Newton coefficients
   double* Ca = ws + Lw.ca_off;
   double* M = ws + Lw.m_off;
   double* Ym = ws + Lw.ym_off;
@@ -474,9 +522,8 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     if constexpr (CERT) { bT[k] = 0.0; bV[k] = 0.0; }
   }
   __syncwarp();
-  if (loop && lane < rows) {
-    st_c(Y + (lane * hp1) * 2, lane < s ? ld_c(Dv + lane * 2) : mkc(0.0, 0.0));  // y_0 = d
-    if constexpr (CERT) Ym[lane * hp1] = lane < s ? ru_abs_c(ld_c(Dv + lane * 2)) : 0.0;
+  if constexpr (CERT) {
+    if (loop && lane < rows) Ym[lane * hp1] = lane < s ? ru_abs_c(ld_c(Dv + lane * 2)) : 0.0;
   }
   // p_1 = tr(C)
   {
@@ -492,12 +539,11 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   }
   __syncwarp();
 
-  // two tile shapes: one 16-row strip with up to 4 column tiles (s <= 16), two
-  // strips with up to 8 (s <= 32); unused tiles are skipped at run time.  Few
-  // shapes keep the instruction footprint small: every subset size runs one of
-  // two code paths.
-  if (s <= 16) haf_powers<4, 1>(Cs, P, Y, Dv, acc_p, s, cs, ps, n, h, loop, lane);
-  else haf_powers<8, 2>(Cs, P, Y, Dv, acc_p, s, cs, ps, n, h, loop, lane);
+  // two tile widths: up to 4 column tiles (s <= 16, one strip) or up to 8 (s <= 32,
+  // two strips in turn); unused tiles are skipped at run time.  Few shapes keep the
+  // instruction footprint small: every subset size runs one of two code paths.
+  if (s <= 16) haf_powers<4>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
+  else haf_powers<8>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
   if constexpr (CERT) {
     __syncwarp();
     if (s <= 16) haf_bound_powers<4, 1>(Ca, M, Ym, Dv, bT, s, cs, ps, n, h, loop, lane);
@@ -505,25 +551,17 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   }
   __syncwarp();
 
-  if (loop) {
-    // v_k = 1/2 sum_i y_a[i^1] y_b[i],  a = (k-1)/2, b = k-1-a: lane k-1 sums over i
-    // (sequentially, in i order) -- one pass for all k instead of a butterfly per k
-    if (lane < n) {
-      const int k = lane + 1;
-      const int aa = (k - 1) >> 1, bb = k - 1 - aa;
-      cplx t = mkc(0.0, 0.0);
-      for (int i = 0; i < s; ++i) t = cadd(t, cmul(ld_c(Y + ((i ^ 1) * hp1 + aa) * 2), ld_c(Y + (i * hp1 + bb) * 2)));
-      st_c(acc_v + 2 * k, cscale(t, 0.5));
-    }
-    for (int k = 1; k <= n; ++k) {
-      const int aa = (k - 1) >> 1, bb = k - 1 - aa;
-      if constexpr (CERT) {
+  if constexpr (CERT) {
+    // loop bound sums V[k] = sum_i Ym[i^1][a] Ym[i][b] (the values v_k came with the powers)
+    if (loop) {
+      for (int k = 1; k <= n; ++k) {
+        const int aa = (k - 1) >> 1, bb = k - 1 - aa;
         double vb = lane < s ? ru_mul(Ym[(lane ^ 1) * hp1 + aa], Ym[lane * hp1 + bb]) : 0.0;
         vb = warp_sum_ru(vb);
         if (lane == 0) bV[k] = vb;
       }
+      __syncwarp();
     }
-    __syncwarp();
   }
 
   // ---- Newton recurrence (lane 0), then broadcast through shared memory
@@ -535,8 +573,9 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       const double sq2 = 1.4142135623730952;
       const double g64 = ru_mul(sq2, gamma_ru(64.0, kU));
       const double gy = ru_mul(sq2, gamma_ru((double)(s + 4), kU));
-      // loop term: complex products (4u) summed sequentially over s rows
-      // (sqrt(2) gamma_{s+4} <= gamma_{2s+8} per component pair)
+      // loop term: complex products (4u) summed sequentially over the rows of each
+      // strip, then the strips (at most s + 1 sums; sqrt(2) gamma_{s+4} <= gamma_{2s+8}
+      // per component pair)
       const double gv = ru_add(4.0 * kU, gamma_ru(2.0 * s + 8.0, kU));
       double ca[kHafMaxPow + 2], ph[kHafMaxPow + 2], ka[kHafMaxPow + 2];
       ca[0] = 0.0; ph[0] = 1.0; ca[1] = 0.0; ph[1] = 1.0;
@@ -581,43 +620,34 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       }
       st_c(ev + 2 * n, e[n].z);
       eb[0] = e[n].r;
-    } else if (slot) {
+    } else {
       st_c(slot, mkc(((n - m) & 1) ? -1.0 : 1.0, 0.0));
       for (int k = 1; k <= n; ++k) {
         cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
         if (loop) g = cadd(g, cscale(ld_c(acc_v + 2 * k), (double)k));
         st_c(slot + 2 * k, g);
       }
-    } else {
-      for (int k = 1; k <= n; ++k) {
-        cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
-        if (loop) g = cadd(g, cscale(ld_c(acc_v + 2 * k), (double)k));
-        st_c(kg + 2 * k, g);
-      }
-      st_c(ev, mkc(1.0, 0.0));
-      for (int j = 1; j <= n; ++j) {
-        cplx acc = mkc(0.0, 0.0);
-        for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(ld_c(kg + 2 * k), ld_c(ev + 2 * (j - k))));
-        st_c(ev + 2 * j, mkc(acc.re / j, acc.im / j));
-      }
     }
   }
   __syncwarp();
-  if (!CERT && slot) return cball{mkc(0.0, 0.0), 0.0};
-  cplx coeff = ld_c(ev + 2 * n);
-  double rad = 0.0;
-  if constexpr (CERT) rad = eb[0];
-  __syncwarp();
-  return cball{((n - m) & 1) ? cneg(coeff) : coeff, rad};
+  if constexpr (!CERT) {
+    return cball{mkc(0.0, 0.0), 0.0};
+  } else {
+    cplx coeff = ld_c(ev + 2 * n);
+    const double rad = eb[0];
+    __syncwarp();
+    return cball{((n - m) & 1) ? cneg(coeff) : coeff, rad};
+  }
 }
 
 // Run the Newton recurrence of `cnt` parked subsets, one lane each, and return
 // the sum of their signed terms (every lane gets it; fixed butterfly order) and,
 // in *absacc, the sum of |term|.
-__device__ __forceinline__ cplx haf_ring_flush(const double* ring, int cnt, int n, int lane, double* absacc) {
+__device__ __forceinline__ cplx haf_ring_flush(const double* ring, int slotw, int cnt, int n, int lane,
+                                               double* absacc) {
   cplx term = mkc(0.0, 0.0);
   if (lane < cnt) {
-    const double* sl = ring + lane * kHafRingSlot * 2;
+    const double* sl = ring + lane * slotw * 2;
     const double sign = sl[0];
     if (sign != 0.0) {
       cplx e[kHafMaxPairs + 1];

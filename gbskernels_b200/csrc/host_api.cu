@@ -674,6 +674,11 @@ static cudaError_t plan_enqueue(gbs_session* s, cudaStream_t stream) {
   for (auto& G : s->groups) {
     if (e != cudaSuccess) break;
     e = launch_any(G.br, G.L, G.grid, G.warps, stream);
+    if (e != cudaSuccess)
+      g_last_error = std::string("work item kernel (branch set ") + std::to_string(G.br) + ", grid " +
+                     std::to_string(G.grid) + " x " + std::to_string(G.warps) + " warps, " +
+                     std::to_string((size_t)G.warps * G.L.ws_doubles * sizeof(double)) + " B shared): " +
+                     cudaGetErrorString(e);
   }
   return e;
 }
@@ -704,9 +709,10 @@ static int plan_launch(gbs_session* s, cudaStream_t stream, bool allow_graph = f
     }
   }
   cudaEventRecord(s->ev0, stream);
+  g_last_error.clear();
   if (graph_now) e = cudaGraphLaunch(s->graph, stream);
   else e = plan_enqueue(s, stream);
-  if (e != cudaSuccess) return fail(e, "launching the work item kernel");
+  if (e != cudaSuccess) return fail(e, "launching the " + (g_last_error.empty() ? std::string("work item kernel") : g_last_error));
   cudaEventRecord(s->ev1, stream);
   s->plan_runs += 1;
   s->last_launches = (int)s->groups.size();
