@@ -40,6 +40,10 @@ struct WorkItem {       // 24 bytes
   unsigned long long count;  // number of subsets / Gray indices / prefix patterns
 };
 
+// log2 of the subsets per hafnian / loop-hafnian work item in the binary64 tiers
+// (the planner and the allocation-free entry share it, so values agree bit for bit)
+constexpr int kHafItemLog2 = 7;
+
 // Branch sets compiled into an item kernel (bit ft_code).  A launch uses the
 // smallest compiled set covering the (function, tier) pairs of its batch.
 constexpr unsigned br1(int fn, int tier) { return 1u << ft_code(fn, tier); }

@@ -223,8 +223,8 @@ static int plan_instance(Plan& P, int fn, int tier, int dim_eval, bool real_in, 
   } else if (fn == kFnHaf || fn == kFnLhaf) {
     const int n = dim_eval / 2;
     const unsigned long long masks = 1ull << n;
-    // masks per item: 2^7 (binary64 tiers) / 2^6 (double-double); smaller instances are one item
-    int per = (tier == kTierDD || tier == kTierCertDD) ? std::min(n, 6) : std::min(n, 7);  // dd tiers: one split
+    // masks per item: 2^kHafItemLog2 (binary64 tiers) / 2^6 (double-double); smaller instances are one item
+    int per = (tier == kTierDD || tier == kTierCertDD) ? std::min(n, 6) : std::min(n, kHafItemLog2);  // dd tiers: one split
     const int tl = tuned_split(fn, tier, dim_eval);
     if (tl >= 0) per = std::min(n, tl);
     const unsigned long long cnt = 1ull << per;

@@ -97,7 +97,7 @@ int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void*
     return (int)cudaMemcpyAsync(d_out, g_h_ones, (size_t)batch * 16, cudaMemcpyHostToDevice, st);
   }
   const int n = N / 2;
-  int per = n < 7 ? n : 7;  // the planner's decomposition (bit-identical results)
+  int per = n < kHafItemLog2 ? n : kHafItemLog2;  // the planner's decomposition (bit-identical results)
   const int tl = tuned_split(kFnHaf, kTierFp64, N);
   if (tl >= 0) per = tl < n ? tl : n;
   const long long items_per = 1ll << (n - per);
