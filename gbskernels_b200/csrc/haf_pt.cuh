@@ -114,7 +114,9 @@ template <int NT, int MS>
 __device__ __forceinline__ void power_product(const double* __restrict__ P, const double* __restrict__ Cs, int s,
                                               int cs, int ps, int ntn, int lane, double (&D)[MS][NT][4]) {
   // P: the previous power (A operand, row stride ps complex); Cs: C (B' source, stride cs)
-  constexpr int KS2 = (MS == 1 && NT <= 4) ? 2 : 1;  // few tiles: split K so eight mma chains are in flight
+  // one accumulator chain per tile for every tile width: the 4- and 8-tile code paths
+  // then give bit-identical results for the subsets both can run (s <= 16)
+  constexpr int KS2 = 1;
   const int g = lane >> 2, t4 = lane & 3;
   double acc[KS2][MS][NT][4];
 #pragma unroll
@@ -539,12 +541,15 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   }
   __syncwarp();
 
-  // ONE tile width for every subset size (up to 8 column tiles, unused ones skipped
-  // at run time; s > 16 runs two strips in turn): a single code path keeps the
-  // instruction footprint within the instruction cache, which measured faster than
-  // a narrower second instantiation for s <= 16 (instruction-fetch stalls fell from
-  // 2.2 to 0.3 cycles per issue).
-  haf_powers<8>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
+  // ONE tile width per launch: up to 4 column tiles when every matrix of the launch
+  // has N <= 16 (every subset fits one strip), otherwise up to 8 for every subset
+  // (unused tiles skipped at run time; s > 16 runs two strips in turn).  A single
+  // hot code path keeps the instruction footprint within the instruction cache:
+  // mixing the two widths in one launch measured slower (instruction-fetch stalls
+  // 2.2 against 0.3 cycles per issue).  Both widths run the same operations on the
+  // tiles in use, so a value does not depend on the launch it is part of.
+  if (Lw.smax <= 16) haf_powers<4>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
+  else haf_powers<8>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
   if constexpr (CERT) {
     __syncwarp();
     if (s <= 16) haf_bound_powers<4, 1>(Ca, M, Ym, Dv, bT, s, cs, ps, n, h, loop, lane);

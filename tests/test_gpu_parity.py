@@ -256,6 +256,18 @@ def test_queue_mixed_equals_alone_bitwise(gpu):
     assert np.array_equal(mixed, per_size)
 
 
+def test_wide_launch_equals_narrow_alone_bitwise(gpu):
+    # a launch whose largest hafnian has N > 16 runs every subset on the 8-tile code
+    # path, one with N <= 16 on the 4-tile path: the values must not depend on it
+    funcs = ["haf", "lhaf", "haf", "lhaf", "haf"]
+    mats = [sym(6), sym(11), sym(16), sym(14), sym(22)]
+    precs = ["fp64", "fp64", "certified", "kappa", "fp64"]
+    with gpu.Workspace() as ws:
+        mixed = ws.evaluate(funcs, mats, precs)
+        alone = np.array([ws.evaluate([f], [m], [p])[0] for f, m, p in zip(funcs, mats, precs)])
+    assert np.array_equal(mixed, alone)
+
+
 def test_workspace_ragged_order_and_reuse(gpu):
     dims = [4, 6, 4, 8, 6, 4, 8]
     mats = [sym(d) for d in dims]
