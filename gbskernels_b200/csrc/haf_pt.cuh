@@ -240,12 +240,13 @@ __device__ __forceinline__ void store_acc(double* P, int ps, int s, int lane, co
 // Lane partial of sum_{i,t} D[i][t] * D[i^1][t^1] (partner in lane ^ 5, same slot).
 // (four independent accumulators: rows g / g + 8 x even / odd tiles)
 template <int NT, int MS>
-__device__ __forceinline__ cplx even_partial(const double (&D)[MS][NT][4]) {
+__device__ __forceinline__ cplx even_partial(const double (&D)[MS][NT][4], int ntn = NT) {
   cplx acc[4] = {mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0)};
 #pragma unroll
   for (int ms = 0; ms < MS; ++ms)
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
+      if (nt >= ntn) continue;  // tiles beyond the matrix are zero (warp-uniform)
       const double p0 = shfl_xor_d(D[ms][nt][0], 5), p1 = shfl_xor_d(D[ms][nt][1], 5);
       const double p2 = shfl_xor_d(D[ms][nt][2], 5), p3 = shfl_xor_d(D[ms][nt][3], 5);
       acc[2 * (nt & 1)] = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), mkc(p0, p1), acc[2 * (nt & 1)]);
@@ -421,7 +422,7 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
     // power 1 (= the strip of C, read in place with stride cs): p_2 and y_1
     load_acc<NT, 1>(Cstrip, cs, s, lane, D);
     {
-      const cplx t = even_partial<NT, 1>(D);
+      const cplx t = even_partial<NT, 1>(D, ntn);
       const double tot = warp_sum4_scatter(t.re, t.im, 0.0, 0.0, lane);
       if (vlead && vq < 2 && 2 <= n) acc_p[4 + vq] += tot;
     }
@@ -432,7 +433,7 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
       const int qs = (a == 2) ? cs : ps;
       power_product<NT, 1>(Q, Cs, s, cs, qs, ntn, lane, D);
       const cplx to = odd_partial<NT, 1>(D, Q, qs, s, lane);
-      const cplx te = even_partial<NT, 1>(D);
+      const cplx te = even_partial<NT, 1>(D, ntn);
       const double tot = warp_sum4_scatter(to.re, to.im, te.re, te.im, lane);
       if (vlead) {
         const int k = vq < 2 ? 2 * a - 1 : 2 * a;
@@ -570,9 +571,10 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     }
   }
 
-  // ---- Newton recurrence (lane 0), then broadcast through shared memory
+  // ---- Newton recurrence (certified: lane 0, then broadcast through shared memory;
+  // binary64 tiers: kg_k parked by lane k, the recurrence runs in haf_ring_flush)
   double* eb = bT;  // reused after the bounds are folded into kg (certified tier)
-  if (lane == 0) {
+  if (!CERT || lane == 0) {
     if constexpr (CERT) {
       // value-path coefficients: E_a <= c_a M_a with M_a = |C|^a, M_a <= phi_a M^_a
       const double g2s = gamma_ru((double)(2 * s), 2.0 * kU);  // FP64 MMA, faithful rounding
@@ -627,8 +629,9 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       st_c(ev + 2 * n, e[n].z);
       eb[0] = e[n].r;
     } else {
-      st_c(slot, mkc(((n - m) & 1) ? -1.0 : 1.0, 0.0));
-      for (int k = 1; k <= n; ++k) {
+      if (lane == 0) st_c(slot, mkc(((n - m) & 1) ? -1.0 : 1.0, 0.0));
+      if (lane >= 1 && lane <= n) {
+        const int k = lane;
         cplx g = cscale(ld_c(acc_p + 2 * k), 0.5);
         if (loop) g = cadd(g, cscale(ld_c(acc_v + 2 * k), (double)k));
         st_c(slot + 2 * k, g);

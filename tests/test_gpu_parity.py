@@ -259,8 +259,14 @@ def test_queue_mixed_equals_alone_bitwise(gpu):
 def test_wide_launch_equals_narrow_alone_bitwise(gpu):
     # a launch whose largest hafnian has N > 16 runs every subset on the 8-tile code
     # path, one with N <= 16 on the 4-tile path: the values must not depend on it
+    rng = np.random.default_rng(2024)  # local: the module stream feeds the other tests
+
+    def lsym(N, scale=0.5):
+        X = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+        return scale * (X + X.T) / 2
+
     funcs = ["haf", "lhaf", "haf", "lhaf", "haf"]
-    mats = [sym(6), sym(11), sym(16), sym(14), sym(22)]
+    mats = [lsym(6), lsym(11), lsym(16), lsym(14), lsym(22)]
     precs = ["fp64", "fp64", "certified", "kappa", "fp64"]
     with gpu.Workspace() as ws:
         mixed = ws.evaluate(funcs, mats, precs)
@@ -308,7 +314,9 @@ def test_tor_complex_vs_binary128_oracle(gpu, orc, n):
     for i in range(2):
         truth, absn = orc.tor(mats[i], "quad", with_absnorm=True)
         kappa = absn / abs(truth)  # sum |term| / |tor|
-        assert rel_err(got[i], truth) < max(FP64_TOL, 1e-15 * kappa), (n, i, kappa)
+        # each term is a subset LU of a 2m x 2m minor (m <= n): O(n) roundings, so
+        # the binary64 sum carries up to ~ n u kappa relative error
+        assert rel_err(got[i], truth) < max(FP64_TOL, 4 * n * 2.2e-16 * kappa), (n, i, kappa)
         if kappa < 1e8:  # the auto tier keeps the binary64 value (no double-double rerun)
             v, d = gpu.tor_batched(mats[i:i + 1], precision="auto", return_diagnostics=True)
             assert v[0] == got[i] and d[0]["tier"] == "fp64"
