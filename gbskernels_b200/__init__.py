@@ -414,7 +414,7 @@ def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: b
         name = "gbs_tor_single_ddcertified_host" if dd else "gbs_tor_single_certified_host"
         fn = getattr(lib, name, None)
         if fn is None:
-            raise RuntimeError(f"tor_single({tier}) is not in this build")
+            raise RuntimeError(f"tor_single({tier}): the loaded libgbs_b200.so lacks {name}")
         _lib.check(fn(_lib.dptr(M), n, g, _lib.dptr(v), _lib.dptr(e)), name)
         vv, ee = float(v[0]), float(e[0])
         if not (np.isfinite(vv) and np.isfinite(ee) and ee >= 0.0):
@@ -424,7 +424,7 @@ def tor_single(O: Any, groups: int | None = None, certified: bool = False, dd: b
         return vv, {"tier": tier, "abs_error_bound": ee, "rel_error_bound": rel}
     fn = getattr(lib, "gbs_tor_recursive_single_host", None)
     if fn is None:
-        raise RuntimeError("tor_single is not in this build")
+        raise RuntimeError("tor_single: the loaded libgbs_b200.so lacks gbs_tor_recursive_single_host")
     _lib.check(fn(_lib.dptr(M), n, g, _lib.dptr(v)), "gbs_tor_recursive_single_host")
     vv = float(v[0])
     if not np.isfinite(vv):
