@@ -463,6 +463,14 @@ class _ResidentView:
         return {"shape": (self._n,), "typestr": self._typestr, "data": (base + self._off if base else 0, False),
                 "version": 3}
 
+    def __dlpack__(self, stream=None):
+        from . import _dlpack
+        return _dlpack.capsule(self._owner, self._owner._addr() + self._off, self._n, self._typestr,
+                               self._owner._device())
+
+    def __dlpack_device__(self):
+        return (2, self._owner._device())
+
     def numpy(self) -> np.ndarray:
         out = np.empty(self._n, dtype=self._dtype)
         if self._n:
@@ -488,13 +496,46 @@ class _ResidentResult:
     def __init__(self, ptr: ctypes.POINTER(ctypes.c_double), n: int):
         self._ptr = ptr
         self._n = n
+        self._exports = 0            # live DLPack tensors over this block
+        self._close_pending = False
+        self._dev = None
         self.aux = _ResidentView(self, 16 * n, n, "<f8", np.float64)
         self.status = _ResidentView(self, 24 * n, n, "<i4", np.int32)
+
+    def _addr(self) -> int:
+        if not self._ptr:
+            raise RuntimeError("resident result is closed")
+        return ctypes.cast(self._ptr, ctypes.c_void_p).value
+
+    def _device(self) -> int:
+        if self._dev is None:
+            d = np.zeros(1, np.int32)
+            _lib.check(_lib.load().gbs_dev_device(ctypes.c_void_p(self._addr()), _lib.iptr(d)), "gbs_dev_device")
+            self._dev = int(d[0])
+        return self._dev
+
+    def _export_acquired(self) -> None:
+        self._exports += 1
+
+    def _export_released(self) -> None:
+        self._exports -= 1
+        if self._exports == 0 and self._close_pending:
+            self._close_pending = False
+            self.close()
 
     @property
     def __cuda_array_interface__(self):
         addr = ctypes.cast(self._ptr, ctypes.c_void_p).value or 0
         return {"shape": (self._n,), "typestr": "<c16", "data": (addr, False), "version": 3}
+
+    def __dlpack__(self, stream=None):
+        """DLPack capsule of the (B,) complex128 values on the device (no copy; the
+        results are complete when the handle is returned, so any stream may read)."""
+        from . import _dlpack
+        return _dlpack.capsule(self, self._addr(), self._n, "<c16", self._device())
+
+    def __dlpack_device__(self):
+        return (2, self._device())  # kDLCUDA
 
     def numpy(self) -> np.ndarray:
         out = np.empty(self._n, dtype=np.complex128)
@@ -509,6 +550,10 @@ class _ResidentResult:
         return self._n
 
     def close(self) -> None:
+        """Release the device block (deferred while DLPack tensors over it are alive)."""
+        if self._exports > 0:
+            self._close_pending = True
+            return
         if self._ptr:
             _lib.load().gbs_dev_free(self._ptr)
             self._ptr = None

@@ -59,6 +59,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_queue_evaluate_resident": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int,
                                      ctypes.POINTER(_dp)], ctypes.c_int),
     "gbs_dev_copy_to_host": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int),
+    "gbs_dev_device": ([_vp, _ip], ctypes.c_int),
     "gbs_dev_to_host": ([_dp, _dp, ctypes.c_int], ctypes.c_int),
     "gbs_dev_free": ([_dp], ctypes.c_int),
     "gbs_queue_evaluate": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int, _dp, _dp, _ip],

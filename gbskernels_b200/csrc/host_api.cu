@@ -1220,6 +1220,15 @@ int gbs_queue_evaluate_resident(gbs_session* s, int B, const int* funcs, const i
   (void)mode;  // results are identical in either launch mode; the persistent queue is used
   return resident_alloc_run(s, reqs, 0, d_block);
 }
+// The device that owns device memory `d` (for DLPack export of resident results).
+int gbs_dev_device(const void* d, int* device) {
+  if (!d || !device) return fail(cudaErrorInvalidValue, "null argument");
+  cudaPointerAttributes at{};
+  const cudaError_t e = cudaPointerGetAttributes(&at, d);
+  if (e != cudaSuccess) return fail(e, "querying a device pointer");
+  *device = at.device;
+  return 0;
+}
 int gbs_dev_copy_to_host(const void* d, void* h, size_t bytes) {
   if (bytes == 0) return 0;
   if (!d || !h) return fail(cudaErrorInvalidValue, "null buffer");

@@ -171,6 +171,8 @@ int gbs_queue_evaluate_resident(gbs_session* s, int B, const int* funcs, const i
                                 const long long* offsets, const double* mats, int mode, double** d_block);
 /* bytes from device memory (a resident block's aux / status parts) to the host */
 int gbs_dev_copy_to_host(const void* d, void* h, size_t bytes);
+/* the CUDA device that owns device memory d (DLPack export of resident results) */
+int gbs_dev_device(const void* d, int* device);
 
 /* ---- ragged, mixed-function, mixed-tier batches ----------------------------
  * reference: gbskernels/__init__.py:813-852 (Workspace._ragged: one launch per

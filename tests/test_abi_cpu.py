@@ -136,3 +136,24 @@ def test_sampler_reduced_A_host_construction():
     assert abs(A[0, 1]) < 1e-12
     with pytest.raises(ValueError):
         sampler.sample_resident(np.eye(10), 4, cutoff=4)  # 2 M cutoff = 40 > 32
+
+
+def test_dlpack_capsule_release_without_consumer():
+    # an unconsumed "dltensor" capsule releases its keep-alive itself
+    import gc
+    from gbskernels_b200 import _dlpack
+
+    class Owner:
+        live = 0
+
+        def _export_acquired(self):
+            Owner.live += 1
+
+        def _export_released(self):
+            Owner.live -= 1
+
+    c = _dlpack.capsule(Owner(), 0x1000, 5, "<c16", 0)
+    assert Owner.live == 1 and len(_dlpack._LIVE) == 1
+    del c
+    gc.collect()
+    assert Owner.live == 0 and not _dlpack._LIVE

@@ -110,3 +110,28 @@ def test_resident_refusals(gpu):
         A[0, 1] = np.inf
         with pytest.raises(ValueError):
             ws.haf_resident(A[None], precision="certified")
+
+
+def test_resident_dlpack_export(gpu):
+    # DLPack (the reference's resident contract): zero-copy tensors over the block;
+    # close() while a tensor is alive is deferred until the tensor is released
+    import gc
+
+    import torch
+    from gbskernels_b200 import _dlpack
+    mats = np.stack([sym(10) for _ in range(4)])
+    with gpu.Workspace() as ws:
+        r = ws.haf_resident(mats, precision="certified")
+        host, bnd = r.numpy(), r.aux.numpy()
+        assert r.__dlpack_device__() == (2, torch.cuda.current_device())
+        t = torch.from_dlpack(r)
+        a = torch.from_dlpack(r.aux)
+        st = torch.from_dlpack(r.status)
+        assert t.dtype == torch.complex128 and a.dtype == torch.float64 and st.dtype == torch.int32
+        assert t.data_ptr() == r.__cuda_array_interface__["data"][0]  # no copy
+        assert np.array_equal(t.cpu().numpy(), host) and np.array_equal(a.cpu().numpy(), bnd)
+        r.close()  # deferred: three tensors still reference the block
+        assert r._ptr and np.array_equal(t.cpu().numpy(), host)
+        del t, a, st
+        gc.collect()
+        assert not r._ptr and not _dlpack._LIVE  # released with the last tensor
