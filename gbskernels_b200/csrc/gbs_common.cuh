@@ -211,8 +211,10 @@ __device__ __forceinline__ double warp_max_d(double v) {
 // (PTX ISA, mma .m16n8k4 .f64):  g = lane/4, t = lane%4;
 //   a0 = A[g][t], a1 = A[g+8][t];  b0 = B[t][g];
 //   c0 = C[g][2t], c1 = C[g][2t+1], c2 = C[g+8][2t], c3 = C[g+8][2t+1].
+// The mma helpers are plain (non-volatile) asm: they have no side effects beyond
+// their outputs, so the compiler may schedule them like arithmetic.
 __device__ __forceinline__ void dmma_m16n8k4(double (&d)[4], double a0, double a1, double b0) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
       : "d"(a0), "d"(a1), "d"(b0));
@@ -222,7 +224,7 @@ __device__ __forceinline__ void dmma_m16n8k4(double (&d)[4], double a0, double a
 // column g): the work of two consecutive m16n8k4 steps in one instruction.
 __device__ __forceinline__ void dmma_m16n8k8(double (&d)[4], double a0, double a1, double a2, double a3, double b0,
                                              double b1) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
       : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
