@@ -955,6 +955,30 @@ static int auto_batch(gbs_session* s, const std::vector<Req>& reqs, double kappa
   return 0;
 }
 
+// Grow a session's plan buffers to hold `mat_bytes` of matrices, `items` work items
+// and `insts` instances up front (the serving slots: a batch within the admission
+// budget then never reallocates -- a device free or a pinned allocation would
+// synchronise the GPU under every slot).
+static int session_reserve(gbs_session* s, size_t mat_bytes, size_t items, size_t insts) {
+  items = std::max<size_t>(items, 1);
+  insts = std::max<size_t>(insts, 1);
+  const size_t meta = insts * sizeof(InstDesc) + items * (sizeof(WorkItem) + sizeof(int)) + 1024;
+  cudaError_t e = grow_pin(s->pin_in, std::max<size_t>(mat_bytes, 16));
+  if (e == cudaSuccess) e = grow_dev(s->mats, std::max<size_t>(mat_bytes, 16), &s->reallocs);
+  if (e == cudaSuccess) e = grow_pin(s->pin_meta, meta);
+  if (e == cudaSuccess) e = grow_dev(s->meta, meta, &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->part, items * 4 * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->paux, items * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->pst, items * sizeof(int), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->done, insts * sizeof(int), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->head, 64 * 8, &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->out, insts * 2 * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->aux, insts * sizeof(double), &s->reallocs);
+  if (e == cudaSuccess) e = grow_dev(s->st, insts * sizeof(int), &s->reallocs);
+  if (e == cudaSuccess) e = grow_pin(s->pin_out, insts * (3 * sizeof(double) + sizeof(int)));
+  return e == cudaSuccess ? 0 : fail(e, "reserving the session buffers");
+}
+
 // Device-resident evaluation of `reqs` into `block` (resident_bytes(B), request
 // order).  tier_mode >= 0: the requests' own tiers; kResidentAuto: fp64 + indicator,
 // the elements with kappa >= kappa_max rerun in double-double and scattered over
@@ -1568,8 +1592,14 @@ int gbs_server_open(int n_slots, long long budget_bytes, int max_batch, gbs_serv
   sv->budget = budget_bytes > 0 ? (size_t)budget_bytes : ((size_t)256 << 20);
   sv->max_batch = max_batch > 0 ? max_batch : 4096;
   sv->slots.resize(n_slots);
+  // per slot, buffers for a batch at the admission budget (req_bytes charges d^2 x 16
+  // bytes of matrix and 48 bytes per work item), so serving never reallocates
+  // (at most 256 MB of matrices per slot up front; a larger budget grows on demand)
+  const size_t rbytes = std::min<size_t>(sv->budget, (size_t)256 << 20);
+  const size_t insts = std::min<size_t>((size_t)sv->max_batch, rbytes / 256 + 1);
   for (Slot& sl : sv->slots) {
     int rc = session_open(&sl.s);
+    if (rc == 0) rc = session_reserve(sl.s, rbytes, rbytes / 48 + 1, insts);
     cudaError_t e = rc == 0 ? cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) : cudaErrorUnknown;
     if (rc || e != cudaSuccess) {
       for (Slot& t : sv->slots) {
