@@ -319,11 +319,12 @@ __global__ void __launch_bounds__(256) gbs_items_kernel(ItemLaunch P) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   double* ws = smem + (size_t)warp * P.ws_doubles;
+  const int n_items = P.n_items_dev ? *P.n_items_dev : P.n_items;
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(P.head, 1);
     it = __shfl_sync(0xffffffffu, it, 0);
-    if (it >= P.n_items) break;
+    if (it >= n_items) break;
     if (P.order) it = P.order[it];
     const WorkItem w = P.items[it];
     const InstDesc d = P.insts[w.inst];

@@ -63,6 +63,7 @@ struct ItemLaunch {
   const WorkItem* items;
   const int* order;        // optional queue order (item indices, heaviest first); null = identity
   int n_items;
+  const int* n_items_dev = nullptr;  // optional: the item count, read on the device (a queue planned there)
   int* head;               // queue head (atomic), zeroed before launch
   int* done;               // per-instance completed-item counters, zeroed before launch
   double* part;            // 4 doubles per item (re_hi, re_lo, im_hi, im_lo)

@@ -3,7 +3,10 @@
 // and the draws' photon-count prefixes, their hafnians evaluated by the work-item
 // kernel (one work item per conditional, the queue planned on the device), and the
 // next photon count drawn by inverse CDF from a counter-based random stream -- no
-// host round trip between modes; only the final counts are read back.
+// host round trip between modes; only the final counts are read back.  Each
+// conditional hafnian is split into work items of 2^7 subsets (the planner's split)
+// by a one-block scan on the device, which also writes the item count the
+// work-item kernel reads: large conditionals spread over many warps.
 // Reference counterpart: core/sampler_gather.cu:20-57 (index rule), core/sampler_draw.cu
 // :15-47 (clip(Re haf, 0) / j! -> normalise -> inverse CDF), core/sampler_session.cu
 // :66-137 (the chain), sampling/sampler.py:214-244 (the host side: A_k and 1/j!).
@@ -13,6 +16,7 @@
 #include <curand_kernel.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -24,13 +28,12 @@ constexpr int kSamplerMaxN = 32;  // the hafnian path's cap (2 M cutoff <= 32)
 
 // One thread per (draw, candidate j): the index list of the host sampler,
 //   [mode i x prefix[i]] + [mode k-1 x j] + [mode i+k x prefix[i]] + [mode 2k-1 x j],
-// and the compact n x n submatrix A_k[idx, idx] at the slot of the instance; the
-// instance's descriptor and single work item (all 2^(n/2) subsets) are written too.
+// and the compact n x n submatrix A_k[idx, idx] at the slot of the instance, with the
+// instance's descriptor (its work items are assigned by sampler_plan_kernel).
 __global__ void __launch_bounds__(128) sampler_gather_kernel(const double* __restrict__ Ak, int k,
                                                              const int* __restrict__ state, int M, int d0,
                                                              int ndraw, int cutoff, int slot, double* __restrict__ sub,
-                                                             InstDesc* __restrict__ insts, WorkItem* __restrict__ items,
-                                                             int* __restrict__ overflow) {
+                                                             InstDesc* __restrict__ insts, int* __restrict__ overflow) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ndraw * (cutoff + 1)) return;
   const int d = d0 + t / (cutoff + 1), j = t % (cutoff + 1);
@@ -71,16 +74,56 @@ __global__ void __launch_bounds__(128) sampler_gather_kernel(const double* __res
   D.off = (long long)t * slot * slot * 2;
   D.dim = n;
   D.ft = ft_code(kFnHaf, kTierFp64);
-  D.item0 = t;
-  D.nitems = 1;
+  D.item0 = 0;
+  D.nitems = 0;
   D.param = 0;
   D.real_in = 0;
   insts[t] = D;
-  WorkItem w{};
-  w.inst = t;
-  w.lo = 0;
-  w.count = 1ull << (n / 2);
-  items[t] = w;
+}
+
+// One block: every instance's work items -- 2^min(n/2, 7) subsets each, in subset
+// order, as the planner splits a hafnian -- at consecutive indices (exclusive scan
+// over the instances in order), and the total item count for the work-item kernel.
+constexpr int kSamplerPlanThreads = 1024;
+__global__ void __launch_bounds__(kSamplerPlanThreads) sampler_plan_kernel(InstDesc* __restrict__ insts, int ni,
+                                                                           WorkItem* __restrict__ items,
+                                                                           int* __restrict__ n_items) {
+  __shared__ long long part[kSamplerPlanThreads];
+  const int tid = threadIdx.x;
+  const int per = (ni + kSamplerPlanThreads - 1) / kSamplerPlanThreads;
+  const int t0 = min(ni, tid * per), t1 = min(ni, t0 + per);
+  auto splits = [&](int t) -> long long {
+    const int h = insts[t].dim / 2;
+    return h > kHafItemLog2 ? (1ll << (h - kHafItemLog2)) : 1;
+  };
+  long long mine = 0;
+  for (int t = t0; t < t1; ++t) mine += splits(t);
+  part[tid] = mine;
+  __syncthreads();
+  // inclusive scan of the thread sums (Hillis-Steele in shared memory)
+  for (int off = 1; off < kSamplerPlanThreads; off <<= 1) {
+    const long long v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  long long base = part[tid] - mine;
+  for (int t = t0; t < t1; ++t) {
+    const int h = insts[t].dim / 2;
+    const int lg = h < kHafItemLog2 ? h : kHafItemLog2;
+    const long long ns = splits(t);
+    insts[t].item0 = (int)base;
+    insts[t].nitems = (int)ns;
+    for (long long q = 0; q < ns; ++q) {
+      WorkItem w{};
+      w.inst = t;
+      w.lo = (unsigned long long)q << lg;
+      w.count = 1ull << lg;
+      items[base + q] = w;
+    }
+    base += ns;
+  }
+  if (tid == kSamplerPlanThreads - 1) *n_items = (int)part[tid];
 }
 
 // One thread per draw: weights clip(Re haf_j, 0) / j!, normalised, inverse CDF with
@@ -154,25 +197,30 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
   SamplerBufs B;
   const int per = cutoff + 1;
   const int slot_max = std::max(2, std::min(kSamplerMaxN, 2 * M * cutoff));
-  // draws per chunk: the slot buffer of one step stays within 1 GiB
-  const size_t slot_bytes = (size_t)per * slot_max * slot_max * 16;
-  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(num_draws, (size_t)(1ull << 30) / slot_bytes));
+  // work items per instance at most (2^7 subsets each)
+  const size_t max_split = (size_t)1 << std::max(0, slot_max / 2 - kHafItemLog2);
+  // draws per chunk: the slots and the item arrays of one step stay within 1 GiB
+  const size_t draw_bytes = (size_t)per * ((size_t)slot_max * slot_max * 16 +
+                                           max_split * (sizeof(WorkItem) + 4 * sizeof(double) + sizeof(double) + sizeof(int)));
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(num_draws, (size_t)(1ull << 30) / draw_bytes));
   const int ninst = chunk * per;
+  const size_t nitem_cap = (size_t)ninst * max_split;
+  if (nitem_cap > (size_t)INT32_MAX) return sampler_fail((int)cudaErrorInvalidValue, "sampler: too many work items");
   cudaError_t e = cudaMalloc(&B.Ak, sizeof(double) * 2 * std::max<long long>(ak_total, 1));
   if (e == cudaSuccess) e = cudaMalloc(&B.invfac, sizeof(double) * per);
   if (e == cudaSuccess) e = cudaMalloc(&B.sub, (size_t)ninst * slot_max * slot_max * 16);
-  if (e == cudaSuccess) e = cudaMalloc(&B.part, sizeof(double) * 4 * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.paux, sizeof(double) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.part, sizeof(double) * 4 * nitem_cap);
+  if (e == cudaSuccess) e = cudaMalloc(&B.paux, sizeof(double) * nitem_cap);
   if (e == cudaSuccess) e = cudaMalloc(&B.out, sizeof(double) * 2 * ninst);
   if (e == cudaSuccess) e = cudaMalloc(&B.aux, sizeof(double) * ninst);
   if (e == cudaSuccess) e = cudaMalloc(&B.state, sizeof(int) * (size_t)num_draws * M);
-  if (e == cudaSuccess) e = cudaMalloc(&B.head, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&B.head, sizeof(int) * 2);  // queue head, item count
   if (e == cudaSuccess) e = cudaMalloc(&B.done, sizeof(int) * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.pst, sizeof(int) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.pst, sizeof(int) * nitem_cap);
   if (e == cudaSuccess) e = cudaMalloc(&B.st, sizeof(int) * ninst);
   if (e == cudaSuccess) e = cudaMalloc(&B.overflow, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&B.insts, sizeof(InstDesc) * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.items, sizeof(WorkItem) * ninst);
+  if (e == cudaSuccess) e = cudaMalloc(&B.items, sizeof(WorkItem) * nitem_cap);
   if (e != cudaSuccess) return sampler_fail((int)e, "sampler: device allocation failed");
   cudaStream_t s = nullptr;
   e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -201,6 +249,7 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
   L.out = B.out;
   L.aux_out = B.aux;
   L.st_out = B.st;
+  L.n_items_dev = B.head + 1;
   L.haf_smax = slot_max;
   L.ws_doubles = (haf_layout(slot_max).total + 3) & ~3;
   int dev = 0, sms = 0;
@@ -220,13 +269,17 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
     for (int k = kfirst; k <= kmax && e == cudaSuccess; ++k) {
       const int slot = std::max(2, std::min(kSamplerMaxN, 2 * k * cutoff));
       sampler_gather_kernel<<<(ni + 127) / 128, 128, 0, s>>>(B.Ak + 2 * (size_t)h_off[k - 1], k, B.state, M, d0, nd,
-                                                            cutoff, slot, B.sub, B.insts, B.items, B.overflow);
+                                                            cutoff, slot, B.sub, B.insts, B.overflow);
       e = cudaGetLastError();
+      if (e == cudaSuccess) {
+        sampler_plan_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.insts, ni, B.items, B.head + 1);
+        e = cudaGetLastError();
+      }
       if (e == cudaSuccess) e = cudaMemsetAsync(B.head, 0, sizeof(int), s);
       if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, sizeof(int) * ni, s);
       if (e == cudaSuccess) {
-        L.n_items = ni;
-        e = launch_br<BR>(L, (int)std::min<long long>((long long)sms * bps, ni), 1, s);
+        L.n_items = (int)nitem_cap;  // upper bound; the kernel reads the planned count
+        e = launch_br<BR>(L, sms * bps, 1, s);
       }
       if (e != cudaSuccess) break;
       if (weights_out && k == kmax) {
