@@ -50,7 +50,7 @@ __host__ __device__ inline HafDDLayout haf_dd_layout(int smax, bool cert = false
   L.total = (L.total + 3) & ~3;  // 32-byte multiple
   L.ca_off = L.m_off = L.ym_off = L.bt_off = L.dv_off = 0;
   if (cert) {
-    const int rows = 16 * haf_strips(smax), cs = haf_c_stride(smax), ps = haf_p_stride(smax);
+    const int rows = 16 * haf_strips(smax), cs = haf_c_stride(smax), ps = haf_p_stride(smax, smax > 16);
     L.ca_off = L.total;
     L.m_off = L.ca_off + rows * cs * 2;
     L.ym_off = L.m_off + rows * ps * 2;
@@ -146,7 +146,7 @@ static __device__ ddball haf_subset_term_dd(const double* __restrict__ A, int N,
     st_ddc(acc_v + 4 * k, ddc_zero());
   }
   // certified: |C| and d in binary64 for the bound path (strides of haf_pt.cuh)
-  const int cs = haf_c_stride(s), ps = haf_p_stride(s), brows = 16 * haf_strips(s);
+  const int cs = haf_c_stride(s), ps = haf_p_stride(s, Lw.smax > 16), brows = 16 * haf_strips(s);
   double* Ca = ws + Lw.ca_off;
   double* M = ws + Lw.m_off;
   double* Ym = ws + Lw.ym_off;

@@ -42,7 +42,14 @@ constexpr int kHafMaxPow = (kHafMaxPairs + 1) / 2;  // h
 
 // Strides (in complex elements) chosen for conflict-free fragment loads.
 __host__ __device__ inline int haf_c_stride(int s) { return ((s + 3) / 8) * 8 + 4; }   // == 4 (mod 8)
-__host__ __device__ inline int haf_p_stride(int s) { return (s % 4 == 2) ? s : s + 2; }  // == 2 (mod 4)
+// The power's row stride, per launch width (it changes no value): the 8-tile path
+// (wide) takes == 4 (mod 8), conflict-free 16-byte stores and odd-trace loads; the
+// 4-tile path == 2 (mod 4), conflict-free 8-byte A-fragment loads, which dominate
+// its small subsets (measured: the wide choice gave the mixed queue +3 %, the narrow
+// one config 1 +2.5 %).
+__host__ __device__ inline int haf_p_stride(int s, bool wide) {
+  return wide ? ((s + 3) / 8) * 8 + 4 : ((s % 4 == 2) ? s : s + 2);
+}
 __host__ __device__ inline int haf_strips(int s) { return (s + 15) / 16; }
 
 // Per-warp shared-memory workspace (doubles), laid out for a launch-wide max s.
@@ -65,7 +72,7 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   HafLayout L;
   if (smax < 2) smax = 2;
   L.smax = smax;
-  const int cs = haf_c_stride(smax), ps = haf_p_stride(smax);
+  const int cs = haf_c_stride(smax), ps = haf_p_stride(smax, smax > 16);
   const int rows = 16 * haf_strips(smax);
   const int h = (smax / 2 + 1) / 2;
   const int np1 = smax / 2 + 1;
@@ -477,7 +484,7 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     return cball{mkc(n == 0 ? 1.0 : 0.0, 0.0), 0.0};
   }
   const int s = 2 * m;
-  const int cs = haf_c_stride(s), ps = haf_p_stride(s);
+  const int cs = haf_c_stride(s), ps = haf_p_stride(s, Lw.smax > 16);
   const int h = (n + 1) / 2, hp1 = h + 1;
   const int rows = 16 * haf_strips(s);
   double* Cs = ws + Lw.c_off;
