@@ -4,6 +4,7 @@
     python -m gbskernels_b200.configs perm20 --tier dd   # 1024 Haar 20x20 permanents
     python -m gbskernels_b200.configs tor --tier certified              # 8192 click patterns, 10..24 modes
     python -m gbskernels_b200.configs tor --batch 64 --kmin 18 --kmax 20  # small case for ncu
+    python -m gbskernels_b200.configs serve              # serving at 1e3 .. 1e5 requests/s
 
 Each run uploads the batch once (a device-resident queue), evaluates it once to
 warm up, then `--reps` more times; the kernel time is the session's own CUDA-event
@@ -11,6 +12,12 @@ time of the last evaluation.  One JSON line: instances/s over the kernel time, t
 launch count, how many instances finished with status ok, and for the certified
 tier the median and maximum relative bound.  `--mode per-size` uses one launch per
 (function, tier, size) bucket instead of the persistent queue.
+
+`serve` replays the chain-rule query stream (haf / lhaf / tor, N 6..30, fp64 70 % /
+auto 20 % / certified 10 %) against the continuous-batching server at each Poisson
+arrival rate of `--rates` (default 1e3, 3e3, 1e4, 3e4, 1e5 requests/s), one JSON
+line per rate: throughput, p50 / p99 latency, and the offline rate of the same
+requests as one batch (measured once).
 """
 
 from __future__ import annotations
@@ -56,7 +63,7 @@ def run(func: str, mats: list, tier: str = "fp64", per_size: bool = False, reps:
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("workload", choices=["haf16", "perm20", "tor"])
+    ap.add_argument("workload", choices=["haf16", "perm20", "tor", "serve"])
     ap.add_argument("--tier", default="fp64", choices=list(_TIER))
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--kmin", type=int, default=10)
@@ -64,7 +71,18 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=None)
     ap.add_argument("--mode", default="persistent", choices=["persistent", "per-size"])
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--rates", default="1e3,3e3,1e4,3e4,1e5")
+    ap.add_argument("--requests", type=int, default=2000)
     a = ap.parse_args(argv)
+    if a.workload == "serve":
+        from .serving import offline_rate, serve_stream
+
+        seed = 5 if a.seed is None else a.seed
+        off = offline_rate(a.requests, seed)
+        for r in (float(x) for x in a.rates.split(",")):
+            res = serve_stream(rate=r, n_req=a.requests, seed=seed, offline=off)
+            print(json.dumps(res), flush=True)
+        return
     if a.workload == "haf16":
         mats = list(workloads.haf_real_batch(a.batch or 4096, 16, seed=1 if a.seed is None else a.seed))
         func = "haf"

@@ -140,20 +140,13 @@ def _pct(x, q):
     return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
 
-def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, rate_frac: float = 0.7,
-                 slots: int = 4, budget_bytes: int = 64 << 20):
-    """Replay a Poisson stream of chain-rule queries (haf / lhaf / tor, N 6..30,
-    fp64 70% / auto 20% / certified 10%) against a Server.
-
-    The offline rate of the same requests (one persistent mixed batch) is measured
-    first; the stream is offered at `rate` requests/s, or at rate_frac x the offline
-    rate when `rate` is None.  Returns throughput, p50/p99 latency, the offline rate
-    and the ratio throughput / offline rate."""
+def offline_rate(n_req: int = 2000, seed: int = 5):
+    """Requests/s of the serving stream's requests evaluated as ONE persistent mixed
+    batch (auto -> its fp64 + indicator pass; the rare double-double reruns are not
+    part of the offline rate), and the batch's values."""
     from . import Workspace
 
     reqs0 = serving_stream(n_req, 1.0, seed=seed)
-    # offline: the same requests as one persistent mixed batch (auto -> its fp64 +
-    # indicator pass; the rare double-double reruns are not part of the offline rate)
     tier_of = {"fp64": "fp64", "auto": "kappa", "certified": "certified"}
     funcs = [r[1] for r in reqs0]
     mats = [r[3] for r in reqs0]
@@ -163,7 +156,23 @@ def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, ra
         t0 = time.perf_counter()
         ws_out = ws.evaluate(funcs, mats, tiers)
         t_off = time.perf_counter() - t0
-    off_rate = n_req / t_off
+    return n_req / t_off, ws_out
+
+
+def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, rate_frac: float = 0.7,
+                 slots: int = 4, budget_bytes: int = 64 << 20, offline=None):
+    """Replay a Poisson stream of chain-rule queries (haf / lhaf / tor, N 6..30,
+    fp64 70% / auto 20% / certified 10%) against a Server.
+
+    The offline rate of the same requests (one persistent mixed batch) is measured
+    first, unless `offline` passes the (rate, values) pair of `offline_rate` for the
+    same n_req and seed; the stream is offered at `rate` requests/s, or at rate_frac
+    x the offline rate when `rate` is None.  Returns throughput, p50/p99 latency, the
+    offline rate, the ratio throughput / offline rate, and the rate at which the
+    submitting thread actually handed the requests over (a Python submit costs tens
+    of microseconds, so the highest offered rates are reached only in bursts)."""
+    reqs0 = serving_stream(n_req, 1.0, seed=seed)
+    off_rate, ws_out = offline if offline is not None else offline_rate(n_req, seed)
     if rate is None:
         rate = rate_frac * off_rate
     gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=n_req)
@@ -180,6 +189,7 @@ def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, ra
             while time.perf_counter() - t_start < ta:
                 pass
             tickets.append(srv.submit(func, mat, prec))
+        t_submitted = time.perf_counter()
         vals = []
         for t in tickets:
             v, info = srv.result(t)
@@ -190,7 +200,8 @@ def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, ra
     thr = n_req / (t_end - t_start)
     fp = [i for i, r in enumerate(reqs) if r[2] in ("fp64", "certified")]
     same = bool(all(vals[i] == ws_out[i] or (np.isnan(vals[i]) and np.isnan(ws_out[i])) for i in fp))
-    return {"offered_rate": rate, "requests": n_req, "throughput": thr, "unit": "requests/s",
+    return {"offered_rate": rate, "submitted_rate": n_req / (t_submitted - t_start),
+            "requests": n_req, "throughput": thr, "unit": "requests/s",
             "p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99), "max_ms": 1e3 * max(lat),
             "offline_rate": off_rate, "throughput_vs_offline": thr / off_rate,
             "batches": stats["batches"], "slots": slots,
