@@ -13,12 +13,11 @@
 // B200 mapping (this repository's own design):
 //   * One warp evaluates one subset at a time; C (s x s complex, s = 2|S|) is
 //     staged in shared memory.
-//   * All 16-row strips of C^a advance together: C^{a+1} = C^a C on the FP64 tensor
-//     cores through the real embedding [Re P, Im P] (interleaved) x B',
-//     B'[2k+p][2j+q] = (p ? iC : C)[k][j] component (q ? im : re): one m16n8k8 mma
-//     consumes four complex columns (an m16n8k4 finishes an odd count); each B'
-//     fragment is loaded once and used by every strip; with few tiles the K loop is
-//     split into two accumulator sets so more independent mma chains are in flight.
+//   * The 16-row strips of C^a run their chains one after the other:
+//     C^{a+1} = C^a C on the FP64 tensor cores through the real embedding
+//     [Re P, Im P] (interleaved) x B', B'[2k+p][2j+q] = (p ? iC : C)[k][j] component
+//     (q ? im : re): one m16n8k8 mma consumes four complex columns (an m16n8k4
+//     finishes an odd count).
 //   * Since C^T = X C X (B_S symmetric), (C^a)^T = X C^a X and
 //       tr(C^{2a})   = sum_{i,t} C^a[i][t]     C^a[i^1][t^1]
 //       tr(C^{2a-1}) = sum_{i,t} C^a[i][t] C^{a-1}[i^1][t^1],
@@ -501,7 +500,7 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   double* bT = ws + Lw.bt_off;                  // trace bound sums T[k]
   double* bV = bT + (kHafMaxPairs + 2);         // loop bound sums V[k]
 
-  // ---- stage C = B_S X, d, and P = C (rows padded to 16 MS with zeros)
+  // ---- stage C = B_S X (rows padded to 16 per strip with zeros) and d
   if (lane < s) {
     uint32_t mm = mask;
     for (int u = 0; u < (lane >> 1); ++u) mm &= mm - 1;
