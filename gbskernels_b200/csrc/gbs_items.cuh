@@ -159,7 +159,8 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
       if (++cnt == kHafRing || k + 1 == w.count) {
         __syncwarp();
         double ab = 0.0;
-        const cplx t = haf_ring_flush(ring, L.slot, cnt, n, lane, TIER == kTierKappa ? &ab : nullptr);
+        const cplx t = haf_ring_flush(ring, L.slot, cnt, n, lane, TIER == kTierKappa ? &ab : nullptr,
+                                      ws + L.p_off);
         acc = cadd(acc, t);
         absacc += ab;
         cnt = 0;

@@ -657,22 +657,27 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
 
 // Run the Newton recurrence of `cnt` parked subsets, one lane each, and return
 // the sum of their signed terms (every lane gets it; fixed butterfly order) and,
-// in *absacc, the sum of |term|.
+// in *absacc, the sum of |term|.  The coefficients e_0..e_n of lane l live in
+// shared memory at e + (j kHafRing + l) complex entries (`e`: (n + 1) kHafRing
+// complex entries that are free while the ring is flushed, the power buffer): a
+// per-thread array would sit in local memory, whose stacks (8.7 KB per warp)
+// overflow the L1 left beside the shared-memory workspaces.
 __device__ __forceinline__ cplx haf_ring_flush(const double* ring, int slotw, int cnt, int n, int lane,
-                                               double* absacc) {
+                                               double* absacc, double* e) {
   cplx term = mkc(0.0, 0.0);
   if (lane < cnt) {
     const double* sl = ring + lane * slotw * 2;
     const double sign = sl[0];
     if (sign != 0.0) {
-      cplx e[kHafMaxPairs + 1];
-      e[0] = mkc(1.0, 0.0);
+      double* el = e + lane * 2;
+      constexpr int es = kHafRing * 2;  // doubles between e_j and e_{j+1} of a lane
+      st_c(el, mkc(1.0, 0.0));
       for (int j = 1; j <= n; ++j) {
         cplx acc = mkc(0.0, 0.0);
-        for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(ld_c(sl + 2 * k), e[j - k]));
-        e[j] = mkc(acc.re / j, acc.im / j);
+        for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(ld_c(sl + 2 * k), ld_c(el + (j - k) * es)));
+        st_c(el + j * es, mkc(acc.re / j, acc.im / j));
       }
-      term = cscale(e[n], sign);
+      term = cscale(ld_c(el + n * es), sign);
     }
   }
   if (absacc) *absacc = warp_sum_d(cabs_fast(term));
