@@ -1,4 +1,4 @@
-"""The decomposition the torontonian walk rests on, checked on the CPU.
+"""The decompositions the torontonian and permanent walks rest on, checked on the CPU.
 
 tor(O) = sum_{S subset [k]} (-1)^(k-|S|) / sqrt(det(I - O)_S)
 (cpu_ref/tor_recursive.py:46-100; xxpp indexing: mode i owns rows i and i + k).
@@ -113,3 +113,45 @@ def test_packed_identity_rows_reproduce_the_compressed_factor_bit_for_bit(r):
             assert [x.hex() for x in piv_p] == [x.hex() for x in piv_c]
             sub = L_p[np.ix_(sel, sel)]
             assert np.array_equal(sub.view(np.uint64), L_c.view(np.uint64))
+
+
+# ---------------------------------------------------------------- permanent
+# The Glynn walk (gbskernels_b200/csrc/perm_tor.cuh) gives each lane an aligned
+# range [i0, i0 + R) of Gray indices: it starts from the row sums at delta(gray(i0))
+# and then flips column ctz(j) + 1 at step j, with the sign of the flip read from
+# gray(i0 + j).  Because i0 is a multiple of R, ctz(i0 + j) = ctz(j): every lane of
+# a warp flips the same column at the same step.
+
+
+def _gray(i: int) -> int:
+    return i ^ (i >> 1)
+
+
+def _lane_range(A: np.ndarray, i0: int, R: int) -> complex:
+    n = A.shape[0]
+    g0 = _gray(i0)
+    delta = np.array([1.0] + [(-1.0 if (g0 >> (c - 1)) & 1 else 1.0) for c in range(1, n)])
+    rs = A @ delta
+    sign = -1.0 if i0 & 1 else 1.0
+    acc = sign * np.prod(rs)
+    for j in range(1, R):
+        i = i0 + j
+        k = (j & -j).bit_length() - 1
+        assert k == (i & -i).bit_length() - 1  # the same column in every lane
+        step = -2.0 if (_gray(i) >> k) & 1 else 2.0
+        rs = rs + step * A[:, k + 1]
+        sign = -sign
+        acc += sign * np.prod(rs)
+    return acc
+
+
+@pytest.mark.parametrize("n,rlog", [(3, 1), (5, 2), (7, 3), (8, 0)])
+def test_aligned_gray_ranges_sum_to_the_permanent(orc, n, rlog):
+    rng = np.random.default_rng(60 + n)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    terms = 1 << (n - 1)
+    R = 1 << min(rlog, n - 1)
+    total = sum(_lane_range(A, i0, R) for i0 in range(0, terms, R))
+    got = total / terms
+    ref = orc.perm(A)
+    assert abs(got - ref) <= 1e-12 * max(abs(ref), 1.0)
