@@ -29,6 +29,19 @@ void t_dd_mul(int n, const double* a, const double* b, double* out) {
     out[2 * i + 1] = r.lo;
   }
 }
+// x / j as the certified Newton recurrence divides (per component): the quotient
+// q = dd_div_d(x, j), the computed product q j and the computed residual x - q j;
+// out holds (q, qj, r) as three double-words per operand.
+void t_dd_div_resid(int n, const double* a, const double* j, double* out) {
+  for (int i = 0; i < n; ++i) {
+    const dd x{a[2 * i], a[2 * i + 1]};
+    const dd q = dd_div_d(x, j[i]);
+    const dd qj = dd_mul_d(q, j[i]);
+    const dd r = dd_sub(x, qj);
+    double* o = out + 6 * i;
+    o[0] = q.hi; o[1] = q.lo; o[2] = qj.hi; o[3] = qj.lo; o[4] = r.hi; o[5] = r.lo;
+  }
+}
 void t_ddc_mul(int n, const double* a, const double* b, double* out) {
   for (int i = 0; i < n; ++i) {
     const double* x = a + 4 * i;

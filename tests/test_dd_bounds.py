@@ -6,6 +6,8 @@ error bound of the double-word routine that produced a value:
   * double-word plus double (dd_add_d):          2u^2 |a + b|
   * double-word product (dd_mul, FMA-based):     5u^2 |a b|
   * complex double-word product (ddc_mul):       21u^2 |x| |y|
+  * division by an integer j (dd_div_d), certified a posteriori from the computed
+    residual r^ = x - (q j)^:  |x - q j| <= |r^| + 4u^2 (|(q j)^| + |r^|)
 (u = 2^-53; Joldes, Muller and Popescu, ACM TOMS 2017, for the first two; the
 product bounds are this repository's expansion for its own FMA ordering).  This
 test compiles the routines of gbskernels_b200/csrc/gbs_common.cuh (the very
@@ -47,7 +49,7 @@ def ddlib():
         subprocess.run(cmd, check=True, capture_output=True)
     lib = ctypes.CDLL(str(out))
     dp = ctypes.POINTER(ctypes.c_double)
-    for name in ("t_dd_add", "t_dd_add_d", "t_dd_mul", "t_ddc_mul"):
+    for name in ("t_dd_add", "t_dd_add_d", "t_dd_mul", "t_ddc_mul", "t_dd_div_resid"):
         getattr(lib, name).argtypes = [ctypes.c_int, dp, dp, dp]
         getattr(lib, name).restype = None
     return lib
@@ -162,3 +164,23 @@ def test_ddc_mul_bound(ddlib):
         err2 = (cr - er) ** 2 + (ci - ei) ** 2
         worst.append(err2 / mod2)
     assert _worst(worst) <= (21 * U ** 2) ** 2, float(_worst(worst) ** 0.5 / U ** 2)
+
+
+def test_division_residual_bound(ddlib):
+    rng = np.random.default_rng(5)
+    x = _dw(rng, N)
+    j = rng.integers(1, 33, N).astype(np.float64)
+    out = np.empty(6 * N)
+    ddlib.t_dd_div_resid(N, _p(x), _p(j), _p(out))
+    worst = []
+    for i in range(N):
+        q = _F(out[6 * i]) + _F(out[6 * i + 1])
+        qj = _F(out[6 * i + 2]) + _F(out[6 * i + 3])
+        r = _F(out[6 * i + 4]) + _F(out[6 * i + 5])
+        err = abs(_val(x, i) - q * _F(j[i]))
+        slack = abs(r) + 4 * U ** 2 * (abs(qj) + abs(r))
+        assert err <= slack, i
+        if abs(qj):
+            worst.append(abs(err - abs(r)) / abs(qj))
+    # the part of the true residual the computed one misses, in units of u^2 |q j|
+    assert _worst(worst) <= 4 * U ** 2, float(_worst(worst) / U ** 2)
