@@ -42,6 +42,27 @@ def test_binding_covers_every_declared_symbol():
     assert not missing
 
 
+def test_binding_arity_matches_the_header():
+    """Every ctypes signature takes as many arguments as its declaration in
+    include/gbs_b200.h (a mismatch would pass garbage through the C ABI)."""
+    import re
+    from gbskernels_b200 import _lib, sampler, serving  # noqa: F401  (both extend SIGNATURES)
+    hdr = (ROOT / "include" / "gbs_b200.h").read_text()
+    hdr = re.sub(r"//[^\n]*", "", hdr)
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    decls = re.findall(r"\b(?:int|const char\s*\*|void|double|long long|size_t)\s+\**\s*(gbs_\w+)\s*\(([^)]*)\)\s*;",
+                       hdr)
+    assert set(n for n, _ in decls) == set(_declared_symbols())
+    bad = []
+    for name, params in decls:
+        p = params.strip()
+        n = 0 if p in ("", "void") else len(p.split(","))
+        argtypes = _lib.SIGNATURES[name][0]
+        if argtypes is not None and len(argtypes) != n:
+            bad.append((name, n, len(argtypes)))
+    assert not bad
+
+
 def test_library_is_sm100a(lib):
     from gbskernels_b200 import build
     assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
