@@ -31,15 +31,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     # value + per-element double (sum|term| or certified bound)
     **{f"gbs_{f}_{k}_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int)
        for f in ("perm", "haf", "lhaf", "tor") for k in ("kappa", "certified")},
-    "gbs_perm_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_haf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_lhaf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_haf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_lhaf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_perm_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_haf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_lhaf_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
-    "gbs_tor_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    # value + certified double-double bound
+    **{f"gbs_{f}_dd_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int)
+       for f in ("perm", "haf", "lhaf", "tor")},
     "gbs_auto_host": ([ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _ip],
                       ctypes.c_int),
     # single-large torontonian

@@ -178,3 +178,27 @@ def test_dlpack_capsule_release_without_consumer():
     del c
     gc.collect()
     assert Owner.live == 0 and not _dlpack._LIVE
+
+
+def test_missing_library_raises_instead_of_falling_back():
+    """Without libgbs_b200.so every GPU entry point raises RuntimeError (no CPU
+    fallback), checked in a fresh interpreter with the library path redirected."""
+    import subprocess
+    import sys
+    code = (
+        "import sys, numpy as np\n"
+        "from pathlib import Path\n"
+        "from gbskernels_b200 import _lib\n"
+        "_lib.LIB_PATH = Path('does-not-exist') / 'libgbs_b200.so'\n"
+        "import gbskernels_b200 as G\n"
+        "for call in (lambda: G.haf(np.eye(4)), lambda: G.perm_batched(np.eye(3)[None]),\n"
+        "             lambda: G.tor(np.zeros((4, 4)))):\n"
+        "    try:\n"
+        "        call()\n"
+        "    except RuntimeError as e:\n"
+        "        assert 'not built' in str(e), e\n"
+        "    else:\n"
+        "        sys.exit('no error')\n"
+        "print('ok')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr[-2000:]
