@@ -202,3 +202,42 @@ def test_missing_library_raises_instead_of_falling_back():
         "print('ok')\n")
     r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr[-2000:]
+
+
+def _header_arity() -> dict:
+    hdr = (ROOT / "include" / "gbs_b200.h").read_text()
+    hdr = re.sub(r"//[^\n]*", "", hdr)
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    out = {}
+    for name, params in re.findall(
+            r"\b(?:int|const char\s*\*|void|double|long long|size_t)\s+\**\s*(gbs_\w+)\s*\(([^)]*)\)\s*;", hdr):
+        p = params.strip()
+        out[name] = 0 if p in ("", "void") else len(p.split(","))
+    return out
+
+
+def test_integration_stub_binds_declared_symbols_with_their_arity(lib):
+    """The ctypes stub a maintainer would drop in as the reference's extension (the
+    python block of INTEGRATION.md) compiles, names only exported symbols, and
+    passes each the number of arguments its declaration takes."""
+    import ast
+    text = (ROOT / "INTEGRATION.md").read_text()
+    blocks = re.findall(r"```python\n(.*?)```", text, flags=re.S)
+    stub = next(b for b in blocks if "gbskernels_ext.py" in b)
+    tree = ast.parse(stub)
+    arity = _header_arity()
+    named = set(re.findall(r'"(gbs_\w+)"', stub))
+    for node in ast.walk(tree):
+        if (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute)
+                and isinstance(node.func.value, ast.Name) and node.func.value.id == "_lib"):
+            name = node.func.attr
+            named.add(name)
+            assert len(node.args) == arity[name], (name, len(node.args), arity[name])
+        # the one-shot batch entries go through _call: (in, dim, batch, out[, aux])
+        if isinstance(node, ast.Call) and isinstance(node.func, ast.Name) and node.func.id == "_call":
+            name = node.args[0].value
+            aux = any(k.arg == "aux" and getattr(k.value, "value", False) for k in node.keywords)
+            assert arity[name] == (5 if aux else 4), name
+    named.discard("gbs_last_error")
+    assert named and all(hasattr(lib, n) for n in named), [n for n in named if not hasattr(lib, n)]
+    assert all(n in arity for n in named)
