@@ -1,4 +1,4 @@
-"""The decompositions the torontonian and permanent walks rest on, checked on the CPU.
+"""The decompositions the torontonian, permanent and sieve walks rest on, checked on the CPU.
 
 tor(O) = sum_{S subset [k]} (-1)^(k-|S|) / sqrt(det(I - O)_S)
 (cpu_ref/tor_recursive.py:46-100; xxpp indexing: mode i owns rows i and i + k).
@@ -155,3 +155,102 @@ def test_aligned_gray_ranges_sum_to_the_permanent(orc, n, rlog):
     got = total / terms
     ref = orc.perm(A)
     assert abs(got - ref) <= 1e-12 * max(abs(ref), 1.0)
+
+
+# ---------------------------------------------------------------- repeated-row sieve
+# The sieve kernel (gbskernels_b200/csrc/k_sieve.cu) walks the digit vectors v of a
+# repetition pattern in reflected mixed-radix Gray order (digit 0 fastest, the
+# largest n_i on top with only floor(n_top / 2) + 1 values: the v <-> n - v
+# symmetry, weight 2 below the middle).  A work item restarts at Gray index t0 from
+# a directly decoded state: per digit q = t0 / place, b = q mod radix, reflected
+# (g = radix - 1 - b) when the parity of q / radix is odd, the top digit never
+# reflected.  A step moves the lowest digit that is not at the end of its run by
+# +-1 (the sign from its reflection parity) and resets the digits below it.
+
+
+def _sieve_digits(reps):
+    modes = [i for i, n in enumerate(reps) if n > 0]
+    modes.sort(key=lambda i: reps[i])  # largest n_i on top (last digit)
+    ns = [int(reps[i]) for i in modes]
+    radix = [n + 1 for n in ns]
+    radix[-1] = ns[-1] // 2 + 1
+    place = [1]
+    for r in radix[:-1]:
+        place.append(place[-1] * r)
+    return modes, ns, radix, place, place[-1] * radix[-1]
+
+
+def _decode(t, radix, place):
+    nd = len(radix)
+    b, par, g = [], [], []
+    for i in range(nd):
+        q = t // place[i]
+        bi = q % radix[i]
+        pi = 0 if i == nd - 1 else (q // radix[i]) & 1
+        b.append(bi)
+        par.append(pi)
+        g.append(radix[i] - 1 - bi if pi else bi)
+    return b, par, g
+
+
+def _step(b, par, g, radix):
+    j = next(i for i in range(len(radix)) if b[i] < radix[i] - 1)
+    d = -1 if par[j] else 1
+    for i in range(j):
+        b[i] = 0
+        par[i] ^= 1
+    b[j] += 1
+    g[j] += d
+    return j, d
+
+
+@pytest.mark.parametrize("reps", [[3], [2, 1], [1, 2, 3], [2, 2, 2, 1], [4, 1, 0, 3]])
+def test_sieve_gray_walk_decodes_steps_and_covers(reps):
+    modes, ns, radix, place, terms = _sieve_digits(reps)
+    seen = set()
+    b, par, g = _decode(0, radix, place)
+    for t in range(terms):
+        assert (b, par, g) == _decode(t, radix, place)  # a restart anywhere agrees
+        seen.add(tuple(g))
+        if t + 1 < terms:
+            prev = list(g)
+            _step(b, par, g, radix)
+            diff = [abs(x - y) for x, y in zip(g, prev)]
+            assert sum(diff) == 1  # one digit, by one
+    assert len(seen) == terms  # every digit vector of the halved box exactly once
+    assert all(0 <= gi <= (n if i < len(ns) - 1 else n // 2) for gi_vec in seen
+               for i, (gi, n) in enumerate(zip(gi_vec, ns)))
+
+
+def _sieve_value(A, gamma, reps):
+    modes, ns, radix, place, terms = _sieve_digits(reps)
+    N = sum(ns)
+    K = N // 2
+    Am = A[np.ix_(modes, modes)]
+    gm = np.asarray(gamma)[modes]
+    tot = 0j
+    b, par, g = _decode(0, radix, place)
+    for t in range(terms):
+        x = np.array([n - 2 * gi for n, gi in zip(ns, g)], dtype=float)
+        s2 = x @ Am @ x
+        mu = x @ gm
+        sn = sum(math.comb(N, 2 * k) * math.prod(range(1, 2 * k, 2)) * s2 ** k * mu ** (N - 2 * k)
+                 for k in range(K + 1))
+        w = 2.0 if 2 * g[-1] < ns[-1] else 1.0
+        sgn = -1.0 if sum(g) & 1 else 1.0
+        tot += sgn * w * math.prod(math.comb(n, gi) for n, gi in zip(ns, g)) * sn
+        if t + 1 < terms:
+            _step(b, par, g, radix)
+    return tot / (math.factorial(N) * 2 ** N)
+
+
+@pytest.mark.parametrize("reps", [[2, 1, 1], [1, 2, 3], [2, 2, 0, 2], [3, 1, 2, 2]])
+def test_sieve_gray_walk_value_equals_the_oracle(orc, reps):
+    rng = np.random.default_rng(sum(reps) * 7 + len(reps))
+    M = len(reps)
+    G = rng.standard_normal((M, M)) + 1j * rng.standard_normal((M, M))
+    A = (G + G.T) / 2
+    gamma = (rng.standard_normal(M) + 1j * rng.standard_normal(M)) * 0.3
+    got = _sieve_value(A, gamma, reps)
+    ref = orc.lhaf_repeated(A, gamma, np.asarray(reps))
+    assert abs(got - ref) <= 1e-10 * max(abs(ref), 1.0)
