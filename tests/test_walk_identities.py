@@ -1,4 +1,5 @@
-"""The decompositions the torontonian, permanent and sieve walks rest on, checked on the CPU.
+"""The decompositions the torontonian, permanent and sieve walks and the subset LU
+rest on, checked on the CPU.
 
 tor(O) = sum_{S subset [k]} (-1)^(k-|S|) / sqrt(det(I - O)_S)
 (cpu_ref/tor_recursive.py:46-100; xxpp indexing: mode i owns rows i and i + k).
@@ -254,3 +255,45 @@ def test_sieve_gray_walk_value_equals_the_oracle(orc, reps):
     got = _sieve_value(A, gamma, reps)
     ref = orc.lhaf_repeated(A, gamma, np.asarray(reps))
     assert abs(got - ref) <= 1e-10 * max(abs(ref), 1.0)
+
+
+# ---------------------------------------------------------------- complex torontonian
+# The subset LU of a complex minor (gbskernels_b200/csrc/tor_lu.cuh) never moves a
+# row: at column c the pivot is the unused row of largest |M[r][c]|^2 (ties: the
+# lowest), and the permutation's parity is accumulated as the number of unused rows
+# below the pivot row, step by step (those are exactly the inversions the pivot
+# contributes).  det = (-1)^parity * prod pivots.
+
+
+def _det_no_swap(M: np.ndarray) -> complex:
+    M = M.astype(np.complex128).copy()
+    m = M.shape[0]
+    used = [False] * m
+    det = 1.0 + 0j
+    inversions = 0
+    for c in range(m):
+        cand = [(abs(M[r, c]) ** 2, -r) for r in range(m) if not used[r]]
+        best, negwho = max(cand)
+        who = -negwho
+        if not best > 0:
+            return 0j
+        inversions += sum(1 for r in range(who) if not used[r])
+        piv = M[who, c]
+        det *= piv
+        used[who] = True
+        for r in range(m):
+            if not used[r]:
+                f = M[r, c] / piv
+                M[r, c + 1:] -= f * M[who, c + 1:]
+    return -det if inversions & 1 else det
+
+
+@pytest.mark.parametrize("m", [1, 2, 5, 8, 12])
+def test_lu_without_row_moves_gives_the_determinant(m):
+    rng = np.random.default_rng(80 + m)
+    for trial in range(20):
+        A = rng.standard_normal((m, m)) + 1j * rng.standard_normal((m, m))
+        if trial % 4 == 0 and m > 1:
+            A[:, 0] = A[0, 0]  # ties in the first pivot column
+        ref = np.linalg.det(A)
+        assert abs(_det_no_swap(A) - ref) <= 1e-10 * max(abs(ref), 1.0)
