@@ -11,11 +11,16 @@
 // file-scope __device__ array of fixed size, kNoAllocScratchBytes (4 MiB), that
 // every GPU loading this library holds until the process exits.
 //
+// The work queue is written on the device by a small fill kernel (each descriptor
+// is a pure function of the instance index, N and the split), which also clears
+// the queue head and the completion counters: no host staging buffer and no
+// host-to-device copy is involved, so nothing the call leaves behind on the host
+// can be read by the GPU later.
+//
 // The result equals gbs_haf_host's bit for bit (same work items, same kernel).
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <cstring>
 #include <mutex>
 
 #include "gbs_items.cuh"
@@ -32,15 +37,48 @@ constexpr int kNoAllocMaxItems = 49152;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// One thread per work item writes its WorkItem; the first item of an instance also
+// writes the InstDesc and clears the instance's completion counter; thread 0 clears
+// the queue head.  Grid-stride, so any grid covers every item.
+__global__ void noalloc_fill_queue(InstDesc* insts, WorkItem* items, int* done, int* head, int batch, int N,
+                                   int per, int items_per) {
+  const long long nit = (long long)batch * items_per;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nit; k += stride) {
+    const int b = (int)(k / items_per);
+    const int j = (int)(k - (long long)b * items_per);
+    WorkItem w{};
+    w.inst = b;
+    w.lo = (unsigned long long)j << per;
+    w.count = 1ull << per;
+    items[k] = w;
+    if (j == 0) {
+      InstDesc d{};
+      d.off = (long long)b * 2 * N * N;
+      d.dim = N;
+      d.ft = ft_code(kFnHaf, kTierFp64);
+      d.item0 = (int)k;
+      d.nitems = items_per;
+      insts[b] = d;
+      done[b] = 0;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0;
+}
+
+// haf of the empty matrix is 1, of an odd-sided one 0: written straight to d_out.
+__global__ void noalloc_fill_trivial(double* out, int batch, double value) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) {
+    out[2 * i] = value;
+    out[2 * i + 1] = 0.0;
+  }
+}
+
 namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_scratch_ptr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
-// host staging of the work queue (static storage: no allocation per call)
-InstDesc g_h_insts[kNoAllocMaxInstances];
-WorkItem g_h_items[kNoAllocMaxItems];
-double g_h_ones[2 * kNoAllocMaxInstances];
 char g_noalloc_err[256] = "";  // static: the error path allocates nothing either
 void set_err(const char* m) { std::snprintf(g_noalloc_err, sizeof(g_noalloc_err), "%s", m); }
 
@@ -74,16 +112,19 @@ extern "C" {
 // row-major, batch-contiguous) already on the device at d_mats, written to d_out
 // (batch complex values), on `stream` (a cudaStream_t; NULL = legacy default).
 // Allocates nothing: the scratch is the fixed 4 MiB array above.
-//  * Limits: N <= 32, batch <= 16384 and at most 49152 work items
-//    (batch x 2^max(0, N/2 - 7)); larger requests return cudaErrorInvalidValue.
+//  * Limits: N <= 32, batch <= 16384 and at most 49152 work items.  The item count
+//    is batch x 2^(N/2 - split) for the split in force for (haf, fp64, N): 7 by
+//    default (so batch x 2^max(0, N/2 - 7)), or the autotuner's value after
+//    gbs_set_split -- the same split gbs_haf_host uses, which keeps the values
+//    equal.  Larger requests return cudaErrorInvalidValue before any launch.
 //  * The first call on a device looks up the scratch array's device address
 //    (cudaGetSymbolAddress, with that device current); make that first call before
 //    any stream capture.
-//  * Every call shares the one array and keeps the last call's contents; calls
-//    whose executions overlap on the GPU (different streams, or threads racing on
-//    one stream) corrupt each other -- serialise them.
-//  * Asynchronous on `stream`; the host staging it copies from is static storage
-//    and calls are serialised by a mutex.
+//  * Every call shares the one array and keeps the last call's contents (the fill
+//    kernel rewrites the queue and clears the counters each call); calls whose
+//    executions overlap on the GPU (different streams, or threads racing on one
+//    stream) corrupt each other -- serialise them.
+//  * Asynchronous on `stream`: two kernel launches, no copies.
 int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void* stream) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   cudaStream_t st = (cudaStream_t)stream;
@@ -91,10 +132,15 @@ int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void*
   if (batch == 0) return 0;
   if (!d_mats || !d_out) { set_err("gbs_haf_noalloc: null device pointer"); return (int)cudaErrorInvalidValue; }
   if (N > kHafMaxN) { set_err("gbs_haf_noalloc: N above 32"); return (int)cudaErrorInvalidValue; }
-  if (N == 0 || (N & 1)) {  // haf of the empty matrix is 1, of an odd one 0
-    if (batch > kNoAllocMaxInstances) { set_err("gbs_haf_noalloc: batch above 16384"); return (int)cudaErrorInvalidValue; }
-    for (int i = 0; i < batch; ++i) { g_h_ones[2 * i] = N == 0 ? 1.0 : 0.0; g_h_ones[2 * i + 1] = 0.0; }
-    return (int)cudaMemcpyAsync(d_out, g_h_ones, (size_t)batch * 16, cudaMemcpyHostToDevice, st);
+  if (batch > kNoAllocMaxInstances) {
+    set_err("gbs_haf_noalloc: batch above 16384");
+    return (int)cudaErrorInvalidValue;
+  }
+  if (N == 0 || (N & 1)) {
+    noalloc_fill_trivial<<<(batch + 255) / 256, 256, 0, st>>>(d_out, batch, N == 0 ? 1.0 : 0.0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) set_err("gbs_haf_noalloc: launch failed");
+    return (int)e;
   }
   const int n = N / 2;
   int per = n < kHafItemLog2 ? n : kHafItemLog2;  // the planner's decomposition (bit-identical results)
@@ -102,10 +148,10 @@ int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void*
   if (tl >= 0) per = tl < n ? tl : n;
   const long long items_per = 1ll << (n - per);
   const long long nit = items_per * batch;
-  if (batch > kNoAllocMaxInstances || nit > kNoAllocMaxItems) {
+  if (nit > kNoAllocMaxItems) {
     std::snprintf(g_noalloc_err, sizeof(g_noalloc_err),
-                  "gbs_haf_noalloc: %d instances / %lld work items exceed the fixed scratch "
-                  "(max 16384 instances, 49152 items)", batch, nit);
+                  "gbs_haf_noalloc: %d instances x %lld items = %lld work items exceed the fixed "
+                  "scratch (max 49152 items)", batch, items_per, nit);
     return (int)cudaErrorInvalidValue;
   }
   void* base = nullptr;
@@ -124,30 +170,11 @@ int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void*
   double* d_aux = (double*)(p + o); o = align256(o + sizeof(double) * batch);
   int* d_st = (int*)(p + o); o = align256(o + sizeof(int) * batch);
   if (o > kNoAllocScratchBytes) { set_err("gbs_haf_noalloc: scratch layout overflow"); return (int)cudaErrorInvalidValue; }
-  // work queue (host static staging -> scratch)
-  long long k = 0;
-  for (int b = 0; b < batch; ++b) {
-    InstDesc d{};
-    d.off = (long long)b * 2 * N * N;
-    d.dim = N;
-    d.ft = ft_code(kFnHaf, kTierFp64);
-    d.item0 = (int)k;
-    d.nitems = (int)items_per;
-    g_h_insts[b] = d;
-    for (long long j = 0; j < items_per; ++j, ++k) {
-      WorkItem w{};
-      w.inst = b;
-      w.lo = (unsigned long long)j << per;
-      w.count = 1ull << per;
-      g_h_items[k] = w;
-    }
-  }
-  e = cudaMemcpyAsync(d_insts, g_h_insts, sizeof(InstDesc) * batch, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_items, g_h_items, sizeof(WorkItem) * nit, cudaMemcpyHostToDevice, st);
-  // the queue head and the completion counters must start at zero every call
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_head, 0, 64, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_done, 0, sizeof(int) * batch, st);
-  if (e != cudaSuccess) { set_err("gbs_haf_noalloc: staging the work queue failed"); return (int)e; }
+  // the work queue, the completion counters and the queue head, written on the device
+  const int fill_grid = (int)std::min<long long>((nit + 255) / 256, 1024);
+  noalloc_fill_queue<<<fill_grid, 256, 0, st>>>(d_insts, d_items, d_done, d_head, batch, N, per, (int)items_per);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { set_err("gbs_haf_noalloc: queue fill launch failed"); return (int)e; }
   ItemLaunch L{};
   L.mats = d_mats;
   L.insts = d_insts;

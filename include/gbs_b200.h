@@ -237,10 +237,13 @@ int gbs_server_stats(gbs_server* sv, long long* completed, long long* batches, l
  * (batch complex) are device pointers the caller owns; every scratch buffer lives
  * in a fixed 4 MiB __device__ array in the library (held by each GPU that loads it
  * until exit).  Limits: N <= 32, batch <= 16384, at most 49152 work items
- * (batch x 2^max(0, N/2 - 7)); larger requests return cudaErrorInvalidValue.  The
- * first call on a device looks up the array's address (call it before any stream
- * capture); calls that overlap on the GPU share the array and race.  Asynchronous
- * on `stream` (a cudaStream_t).  Values equal gbs_haf_host's bit for bit.        */
+ * (batch x 2^(N/2 - split), split = 7 unless gbs_set_split tuned (haf, fp64, N):
+ * batch x 2^max(0, N/2 - 7) by default); larger requests return
+ * cudaErrorInvalidValue.  The work queue is written on the device by a fill
+ * kernel, so no host buffer is read after the call returns.  The first call on a
+ * device looks up the array's address (make it before any stream capture); calls
+ * that overlap on the GPU share the array and race.  Asynchronous on `stream` (a
+ * cudaStream_t).  Values equal gbs_haf_host's bit for bit (same split).         */
 int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void* stream);
 const char* gbs_haf_noalloc_last_error(void);
 
