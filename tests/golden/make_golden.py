@@ -1,8 +1,9 @@
 """Generate tests/golden/golden.npz from the REFERENCE implementation.
 
-Run in a container where the reference tree is mounted (default /root/reference):
+Run where a reference checkout is available, naming it with --ref (or the
+GBS_REFERENCE_DIR environment variable):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference tree>
 
 For seeded small inputs of every function it records
   * the reference's mpmath ground truth (highprec_ref.*_mp, 40 digits) as (hi, lo)
@@ -17,6 +18,7 @@ at test time.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -38,9 +40,12 @@ def _mp_pair(x) -> tuple[float, float, float, float]:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("GBS_REFERENCE_DIR"),
+                    help="reference checkout (default: $GBS_REFERENCE_DIR)")
     ap.add_argument("--out", default=str(HERE / "golden.npz"))
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("name the reference checkout with --ref or GBS_REFERENCE_DIR")
     sys.path.insert(0, args.ref)
     import cpu_ref  # noqa: E402  (reference package)
     import highprec_ref  # noqa: E402

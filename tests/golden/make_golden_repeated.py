@@ -1,6 +1,6 @@
 """Generate tests/golden/golden_repeated.npz from the REFERENCE implementation.
 
-    python tests/golden/make_golden_repeated.py [--ref /root/reference]
+    python tests/golden/make_golden_repeated.py --ref <reference tree>   (or GBS_REFERENCE_DIR)
 
 Seeded repeated-row loop-hafnian cases (base matrix A, loop weights gamma, one
 repetition pattern each; small enough that the expansion's mpmath value is cheap):
@@ -13,6 +13,7 @@ repetition pattern each; small enough that the expansion's mpmath value is cheap
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -23,9 +24,12 @@ HERE = Path(__file__).resolve().parent
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("GBS_REFERENCE_DIR"),
+                    help="reference checkout (default: $GBS_REFERENCE_DIR)")
     ap.add_argument("--out", default=str(HERE / "golden_repeated.npz"))
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("name the reference checkout with --ref or GBS_REFERENCE_DIR")
     sys.path.insert(0, args.ref)
     import mpmath
     import cpu_ref  # noqa: E402  (reference package)
