@@ -216,28 +216,33 @@ def _header_arity() -> dict:
     return out
 
 
-def test_integration_stub_binds_declared_symbols_with_their_arity(lib):
-    """The ctypes stub a maintainer would drop in as the reference's extension (the
-    python block of INTEGRATION.md) compiles, names only exported symbols, and
-    passes each the number of arguments its declaration takes."""
+def test_extension_module_binds_declared_symbols_with_their_arity(lib):
+    """gbskernels_b200/ext/gbskernels_ext.py (the module the reference package
+    imports as its extension) names only exported symbols and passes each the
+    number of arguments its declaration in include/gbs_b200.h takes."""
     import ast
-    text = (ROOT / "INTEGRATION.md").read_text()
-    blocks = re.findall(r"```python\n(.*?)```", text, flags=re.S)
-    stub = next(b for b in blocks if "gbskernels_ext.py" in b)
-    tree = ast.parse(stub)
+    src = (ROOT / "gbskernels_b200" / "ext" / "gbskernels_ext.py").read_text()
+    tree = ast.parse(src)
     arity = _header_arity()
-    named = set(re.findall(r'"(gbs_\w+)"', stub))
+    named = set()
     for node in ast.walk(tree):
-        if (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute)
-                and isinstance(node.func.value, ast.Name) and node.func.value.id == "_lib"):
-            name = node.func.attr
-            named.add(name)
-            assert len(node.args) == arity[name], (name, len(node.args), arity[name])
-        # the one-shot batch entries go through _call: (in, dim, batch, out[, aux])
-        if isinstance(node, ast.Call) and isinstance(node.func, ast.Name) and node.func.id == "_call":
+        if not isinstance(node, ast.Call):
+            continue
+        f = node.func
+        # direct calls: _lib.gbs_x(...)
+        if isinstance(f, ast.Attribute) and isinstance(f.value, ast.Name) and f.value.id == "_lib":
+            named.add(f.attr)
+            if f.attr.startswith("gbs_") and not f.attr.endswith("last_error"):
+                assert len(node.args) == arity[f.attr], (f.attr, len(node.args), arity[f.attr])
+        # table calls: _eval("gbs_x", a) -> (in, dim, batch, out); _eval_aux -> + aux;
+        # _tor_single_bound("gbs_x", O, g) -> (O, n, g, out, bound)
+        if isinstance(f, ast.Name) and f.id in ("_eval", "_eval_aux", "_tor_single_bound") and node.args \
+                and isinstance(node.args[0], ast.Constant):
             name = node.args[0].value
-            aux = any(k.arg == "aux" and getattr(k.value, "value", False) for k in node.keywords)
-            assert arity[name] == (5 if aux else 4), name
-    named.discard("gbs_last_error")
-    assert named and all(hasattr(lib, n) for n in named), [n for n in named if not hasattr(lib, n)]
-    assert all(n in arity for n in named)
+            named.add(name)
+            want = {"_eval": 4, "_eval_aux": 5, "_tor_single_bound": 5}[f.id]
+            assert arity[name] == want, (name, arity[name], want)
+    named = {n for n in named if n.startswith("gbs_")}
+    assert len(named) >= 30
+    assert all(hasattr(lib, n) for n in named), [n for n in named if not hasattr(lib, n)]
+    assert all(n in arity for n in named), [n for n in named if n not in arity]
