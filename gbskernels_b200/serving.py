@@ -142,8 +142,8 @@ def _pct(x, q):
 
 def offline_rate(n_req: int = 2000, seed: int = 5):
     """Requests/s of the serving stream's requests evaluated as ONE persistent mixed
-    batch (auto -> its fp64 + indicator pass; the rare double-double reruns are not
-    part of the offline rate), and the batch's values."""
+    batch of host-gathered matrices (auto -> its fp64 + indicator pass; the rare
+    double-double reruns are not part of the offline rate), and the batch's values."""
     from . import Workspace
 
     reqs0 = serving_stream(n_req, 1.0, seed=seed)
@@ -160,35 +160,54 @@ def offline_rate(n_req: int = 2000, seed: int = 5):
 
 
 def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, rate_frac: float = 0.7,
-                 slots: int = 4, budget_bytes: int = 64 << 20, offline=None):
-    """Replay a Poisson stream of chain-rule queries (haf / lhaf / tor, N 6..30,
-    fp64 70% / auto 20% / certified 10%) against a Server.
+                 slots: int = 4, budget_bytes: int = 64 << 20, offline=None, resident: bool = True):
+    """Replay a Poisson stream of chain-rule sampler queries (haf / lhaf / tor,
+    matrix side 6..30, growing prefixes per chain, fp64 70% / auto 20% / certified
+    10%; workloads.serving_chains) against a Server.
 
-    The offline rate of the same requests (one persistent mixed batch) is measured
-    first, unless `offline` passes the (rate, values) pair of `offline_rate` for the
-    same n_req and seed; the stream is offered at `rate` requests/s, or at rate_frac
-    x the offline rate when `rate` is None.  Returns throughput, p50/p99 latency, the
-    offline rate, the ratio throughput / offline rate, and the rate at which the
-    submitting thread actually handed the requests over (a Python submit costs tens
-    of microseconds, so the highest offered rates are reached only in bursts)."""
-    reqs0 = serving_stream(n_req, 1.0, seed=seed)
+    resident=True (default): the two states (the GBS kernel A with its loop weights,
+    the threshold matrix O_x) are uploaded once with add_state and every query is
+    submitted as (state, index list) -- its submatrix is gathered on the device.
+    resident=False submits the host-gathered matrices instead.
+
+    The offline rate of the same requests (one persistent mixed batch of host
+    matrices) is measured first, unless `offline` passes the (rate, values) pair of
+    `offline_rate` for the same n_req and seed; the stream is offered at `rate`
+    requests/s, or at rate_frac x the offline rate when `rate` is None.  Returns
+    throughput, p50/p99 latency, the offline rate, the ratio throughput / offline
+    rate, whether every fp64 / certified value equals the offline batch's bit for
+    bit, and the rate at which the submitting thread actually handed the requests
+    over (a Python submit costs tens of microseconds, so the highest offered rates
+    are reached only in bursts)."""
+    from .workloads import gather_query, serving_chains
+
+    states, queries = serving_chains(n_req, 1.0, seed=seed)
     off_rate, ws_out = offline if offline is not None else offline_rate(n_req, seed)
     if rate is None:
         rate = rate_frac * off_rate
     gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=n_req)
     arrivals = np.cumsum(gaps)
-    reqs = [(float(arrivals[i]),) + tuple(reqs0[i][1:]) for i in range(n_req)]
     lat = []
     with Server(slots=slots, budget_bytes=budget_bytes) as srv:
-        # warm the slots
-        for r in reqs[:8]:
-            srv.result(srv.submit(r[1], r[3], r[2]))
+        sid = {}
+        if resident:
+            sid["A"] = srv.add_state(states["A"], states["gamma"])
+            sid["O"] = srv.add_state(states["O"])
+
+        def submit(q):
+            _, func, prec, key, idx, ug = q
+            if resident:
+                return srv.submit_state(func, sid[key], idx, prec, use_gamma=ug)
+            return srv.submit(func, gather_query(states, key, idx, ug), prec)
+
+        for q in queries[:8]:  # warm the slots
+            srv.result(submit(q))
         tickets = []
         t_start = time.perf_counter()
-        for (ta, func, prec, mat) in reqs:
-            while time.perf_counter() - t_start < ta:
+        for i, q in enumerate(queries):
+            while time.perf_counter() - t_start < arrivals[i]:
                 pass
-            tickets.append(srv.submit(func, mat, prec))
+            tickets.append(submit(q))
         t_submitted = time.perf_counter()
         vals = []
         for t in tickets:
@@ -198,12 +217,13 @@ def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, ra
         t_end = time.perf_counter()
         stats = srv.stats()
     thr = n_req / (t_end - t_start)
-    fp = [i for i, r in enumerate(reqs) if r[2] in ("fp64", "certified")]
+    fp = [i for i, q in enumerate(queries) if q[2] in ("fp64", "certified")]
     same = bool(all(vals[i] == ws_out[i] or (np.isnan(vals[i]) and np.isnan(ws_out[i])) for i in fp))
     return {"offered_rate": rate, "submitted_rate": n_req / (t_submitted - t_start),
             "requests": n_req, "throughput": thr, "unit": "requests/s",
             "p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99), "max_ms": 1e3 * max(lat),
             "offline_rate": off_rate, "throughput_vs_offline": thr / off_rate,
             "batches": stats["batches"], "slots": slots,
+            "path": "resident states, device gather (submit_state)" if resident else "host matrices (submit)",
+            "stream": "chain-rule queries: growing prefixes, 8 samplers side by side",
             "values_equal_to_offline_batch": same}
-

@@ -117,36 +117,74 @@ def tor_click_batch(B: int = 8192, kmin: int = 10, kmax: int = 24, M: int = 50, 
 
 
 # ---------------------------------------------------------------- config 5
-def serving_stream(n_req: int, rate: float, seed: int = 5, M: int = 50, nmin: int = 6, nmax: int = 30):
-    """Poisson arrivals of chain-rule sampler queries: (arrival_s, func, precision,
-    matrix).  func in {haf, lhaf, tor}; n = matrix side uniform over even values in
-    [nmin, nmax] (tor: n/2 modes); precision fp64 70% / auto 20% / certified 10%;
-    matrices are growing submatrices of resident states."""
+def serving_chains(n_req: int, rate: float, seed: int = 5, M: int = 50, nmin: int = 6, nmax: int = 30,
+                   lanes: int = 8):
+    """Poisson arrivals of chain-rule sampler queries on resident states.
+
+    States: the pure-state GBS kernel A = U diag(tanh 1) U^T (M x M) with loop
+    weights gamma ~ CN(0, 0.1), and the threshold-detector matrix O_x (2M x 2M, xxpp)
+    of a lossy squeezed state.  `lanes` samplers run side by side; each runs chains
+    one after another, and a chain is the sequence of growing submatrices a
+    chain-rule sampler evaluates as it extends its pattern: for haf / lhaf the
+    prefixes of a sorted photon pattern (repeated modes; two photons more per step,
+    sizes up to n_final uniform over the even values in [nmin, nmax]), for tor the
+    click-set prefixes (one mode more per step, matrix side 2k).  Arrival i is the
+    next query of lane i mod `lanes`.  Precision per query: fp64 70 % / auto 20 % /
+    certified 10 %.
+
+    Returns (states, queries): states = {"A": A, "gamma": gamma, "O": O_x};
+    queries = [(arrival_s, func, precision, state_key, idx, use_gamma)], the matrix
+    of a query being state[idx][:, idx] (with gamma[idx] on the diagonal when
+    use_gamma)."""
     rng = np.random.default_rng(seed)
     A = gbs_kernel(M, 1.0, seed)
     gamma = (rng.standard_normal(M) + 1j * rng.standard_normal(M)) * np.sqrt(0.05)
     Ox = threshold_O(lossy_squeezed_cov(M, seed=seed))
     t = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
-    out = []
     sizes = np.arange(nmin, nmax + 1, 2)
-    for i in range(n_req):
+
+    def new_chain():
         func = ["haf", "lhaf", "tor"][int(rng.integers(0, 3))]
+        steps = int(rng.integers(1, 5))
+        nf = int(rng.choice(sizes))
+        if func == "tor":
+            kf = nf // 2
+            S = np.sort(rng.choice(M, size=kf, replace=False))
+            k0 = max(nmin // 2, kf - steps + 1)
+            return [(func, "O", np.concatenate([S[:k], S[:k] + M]).astype(np.int32), False)
+                    for k in range(k0, kf + 1)]
+        idx = np.sort(rng.integers(0, M, size=nf)).astype(np.int32)
+        n0 = max(nmin, nf - 2 * (steps - 1))
+        return [(func, "A", idx[:n].copy(), func == "lhaf") for n in range(n0, nf + 1, 2)]
+
+    pending = [[] for _ in range(lanes)]
+    queries = []
+    for i in range(n_req):
+        lane = i % lanes
+        if not pending[lane]:
+            pending[lane] = new_chain()
+        func, key, idx, ug = pending[lane].pop(0)
         u = rng.random()
         prec = "fp64" if u < 0.7 else ("auto" if u < 0.9 else "certified")
-        n = int(rng.choice(sizes))
-        if func == "tor":
-            k = n // 2
-            S = np.sort(rng.choice(M, size=k, replace=False))
-            idx = np.concatenate([S, S + M])
-            mat = np.ascontiguousarray(Ox[np.ix_(idx, idx)]).astype(np.complex128)
-        else:
-            idx = np.sort(rng.integers(0, M, size=n))
-            mat = np.ascontiguousarray(A[np.ix_(idx, idx)])
-            if func == "lhaf":
-                mat = mat.copy()
-                np.fill_diagonal(mat, gamma[idx])
-        out.append((float(t[i]), func, prec, mat))
-    return out
+        queries.append((float(t[i]), func, prec, key, idx, ug))
+    return {"A": A, "gamma": gamma, "O": Ox}, queries
+
+
+def gather_query(states: dict, key: str, idx: np.ndarray, use_gamma: bool) -> np.ndarray:
+    """The matrix of a resident-state query, gathered on the host: state[idx][:, idx]
+    (gamma[idx] on the diagonal when use_gamma), complex128."""
+    S = np.ascontiguousarray(np.asarray(states[key], dtype=np.complex128)[np.ix_(idx, idx)])
+    if use_gamma:
+        np.fill_diagonal(S, states["gamma"][idx])
+    return S
+
+
+def serving_stream(n_req: int, rate: float, seed: int = 5, M: int = 50, nmin: int = 6, nmax: int = 30):
+    """The chain-rule query stream of `serving_chains` with every matrix gathered on
+    the host: [(arrival_s, func, precision, matrix)] (the host-matrix form of the
+    same requests, for servers fed explicit matrices and for offline batches)."""
+    states, queries = serving_chains(n_req, rate, seed=seed, M=M, nmin=nmin, nmax=nmax)
+    return [(ta, f, p, gather_query(states, k, idx, ug)) for (ta, f, p, k, idx, ug) in queries]
 
 
 # ---------------------------------------------------------------- algorithmic work

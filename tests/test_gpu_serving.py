@@ -80,3 +80,14 @@ def test_server_rejects_bad_requests(gpu):
             srv.submit_state("haf", sid, [0, 9])
         with pytest.raises(RuntimeError):
             srv.submit_state("lhaf", sid, [0, 1], use_gamma=True)  # no loop weights uploaded
+
+
+def test_chain_rule_stream_from_resident_states(gpu):
+    """The serving benchmark's path: chain-rule queries (growing prefixes) on two
+    resident states, gathered on the device, values bit-identical to the offline
+    batch of host-gathered matrices, at a rate that keeps several batches in flight."""
+    from gbskernels_b200.serving import serve_stream
+    res = serve_stream(rate=2e4, n_req=400, seed=13, slots=3)
+    assert res["values_equal_to_offline_batch"], res
+    assert res["path"].startswith("resident")
+    assert res["batches"] > 3 and res["p99_ms"] >= res["p50_ms"] > 0
