@@ -16,6 +16,20 @@ weights gamma ~ CN(0, 0.1) on the loop-hafnian diagonals (gbskernels_b200.worklo
            FP64 tensor-core peak measured live by gbs_probe_fp64_peak
   cpu_baseline    the oracle (binary64 restatement of the reference algorithm) on the
            host cores, stratified sample: one haf + one lhaf instance per size class
+  plain_per_size_sync  the reference's plain per-size path (gbskernels/__init__.py:
+           813-852 over core/host_api.cu:537-590): one synchronous session call per
+           (function, size) bucket -- stack, H2D, launch, D2H, sync -- and a host
+           scatter, end to end from numpy, against this library's e2e
+  batch_sweep     the persistent queue against both per-size paths at 256..16384
+           instances of the same mix (where one launch per size underfills the GPU)
+  configs  the other benchmark configurations, each on its own batch: real 16 x 16
+           hafnians (fp64, certified), Haar 20 x 20 permanents (fp64, dd), threshold
+           torontonians at 10..24 modes (fp64, certified), with parity spot checks
+  serving  the chain-rule query stream from resident states at 0.75 x and 3 x the
+           offline rate (the second saturates: its throughput is the capacity)
+  check    one haf + one lhaf instance per size class 8..28 of this batch against
+           the binary128 oracle (N <= 20) or the binary64 oracle port scaled by the
+           instance's cancellation indicator (N >= 22)
 
 Multi-GPU (torchrun): replicas only -- each rank evaluates its own batch (weak
 scaling), no collective on the data path; the barrier and the max-over-ranks time
@@ -59,6 +73,8 @@ def _args():
     ap.add_argument("--no-per-size", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--tuned", default=None,
                     help="apply an autotuner table (gbskernels_b200.autotune JSON) before timing")
     ap.add_argument("--profile-small", action="store_true",
@@ -224,6 +240,180 @@ def run_reference(a, dist: Dist):
     print(json.dumps(line), flush=True)
 
 
+
+# ---------------------------------------------------------------- parity spot check
+def _check_task(args):
+    func, mat, prec = args
+    sys.path.insert(0, str(ROOT))
+    import oracle
+    if prec == "quad":
+        return complex(getattr(oracle, func)(mat, "quad")), None
+    v, absn = getattr(oracle, func)(mat, "fp64", with_absnorm=True)
+    return complex(v), float(absn)
+
+
+def parity_check(funcs, mats, out, cores):
+    """One haf + one lhaf per size class against the oracle: binary128 for N <= 20,
+    the binary64 port above with the tolerance max(1e-10, 16 N u kappa), kappa the
+    port's sum|term| / |value| (both walks err by about N u kappa)."""
+    picked = {}
+    for i, (f, m) in enumerate(zip(funcs, mats)):
+        picked.setdefault((f, m.shape[0]), i)
+    idx = sorted(picked.values(), key=lambda i: -mats[i].shape[0])
+    tasks = [(funcs[i], mats[i], "quad" if mats[i].shape[0] <= 20 else "fp64") for i in idx]
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(min(cores, len(tasks))) as pool:
+        res = pool.map(_check_task, tasks, chunksize=1)
+    worst_q, worst_p, ok = 0.0, 0.0, True
+    for i, (ref, absn) in zip(idx, res):
+        err = abs(out[i] - ref) / abs(ref)
+        if absn is None:
+            worst_q = max(worst_q, err)
+            ok &= err <= 1e-10
+        else:
+            tol = max(1e-10, 16 * mats[i].shape[0] * 2.0 ** -53 * absn / abs(ref))
+            worst_p = max(worst_p, err / tol)
+            ok &= err <= tol
+    return {"instances": len(idx), "max_rel_err_vs_binary128_N<=20": float(worst_q),
+            "max_err_over_tol_vs_binary64_port_N>=22": float(worst_p), "pass": bool(ok)}
+
+
+# ---------------------------------------------------------------- reference-style per-size path
+def per_size_sync(lib, sess, funcs, mats):
+    """The reference's plain per-size path (gbskernels/__init__.py:813-852): group by
+    (function, size) in first-seen order, one synchronous session call per bucket
+    (stack, H2D, launch, D2H, sync: gbs_session_evaluate, as core/host_api.cu:537-590),
+    scatter to input order."""
+    from gbskernels_b200 import _lib
+    buckets: dict = {}
+    for i, (f, m) in enumerate(zip(funcs, mats)):
+        buckets.setdefault((f, m.shape[0]), []).append(i)
+    out = np.empty(len(mats), np.complex128)
+    code = {"perm": 0, "haf": 1, "lhaf": 2, "tor": 3}
+    for (f, d), idxs in buckets.items():
+        stack = np.ascontiguousarray(np.stack([mats[i] for i in idxs]))
+        res = np.empty(len(idxs), np.complex128)
+        _lib.check(lib.gbs_session_evaluate(sess, code[f], 0, _lib.dptr(stack.view(np.float64)), d, len(idxs),
+                                            _lib.dptr(res.view(np.float64))), "gbs_session_evaluate")
+        out[idxs] = res
+    return out
+
+
+def batch_sweep(G, lib, sizes, seed, stream, sptr):
+    """Persistent queue vs the two per-size paths at several batch sizes of the mix."""
+    import torch
+    from gbskernels_b200 import _lib, workloads
+    rows = []
+    for B in sizes:
+        funcs, mats = workloads.mixed_haf_lhaf(B, seed=seed + 100 + B)
+        fcode = np.array([{"haf": 1, "lhaf": 2}[f] for f in funcs], np.int32)
+        tiers = np.zeros(B, np.int32)
+        buf, dims, offs = G._pack(mats)
+        row = {"batch": B}
+        with G.Workspace() as ws, G.Workspace() as ws2:
+            reps = 3 if B <= 4096 else 2
+            for mode, key in ((0, "persistent_ms"), (1, "per_size_ms")):
+                _lib.check(lib.gbs_queue_prepare(ws._session, B, _lib.iptr(fcode), _lib.iptr(tiers), _lib.iptr(dims),
+                                                 _lib.llptr(offs), _lib.dptr(buf.view(np.float64)), mode), "prepare")
+                for _ in range(2):
+                    _lib.check(lib.gbs_queue_run(ws._session, sptr), "run")
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    _lib.check(lib.gbs_queue_run(ws._session, sptr), "run")
+                e1.record(stream)
+                torch.cuda.synchronize()
+                row[key] = e0.elapsed_time(e1) / reps
+            precs = ["fp64"] * B
+            ref = ws.evaluate(funcs, mats, precs)
+            per_size_sync(lib, ws2._session, funcs, mats)  # warm
+            t_e, t_s = [], []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                r1 = ws.evaluate(funcs, mats, precs)
+                t_e.append(time.perf_counter() - t0)
+                t0 = time.perf_counter()
+                r2 = per_size_sync(lib, ws2._session, funcs, mats)
+                t_s.append(time.perf_counter() - t0)
+            row["e2e_persistent_ms"] = 1e3 * float(np.median(t_e))
+            row["e2e_per_size_sync_ms"] = 1e3 * float(np.median(t_s))
+            row["speedup_resident_vs_per_size"] = row["per_size_ms"] / row["persistent_ms"]
+            row["speedup_e2e_vs_per_size_sync"] = row["e2e_per_size_sync_ms"] / row["e2e_persistent_ms"]
+            row["values_equal"] = bool(np.array_equal(r1, ref) and np.array_equal(r2, ref))
+        rows.append(row)
+    return rows
+
+
+# ---------------------------------------------------------------- the other configurations
+def _cfg_task(args):
+    kind, mat = args
+    sys.path.insert(0, str(ROOT))
+    import oracle
+    return complex(getattr(oracle, kind)(mat, "quad"))
+
+
+def other_configs(G, peak, cores):
+    """Configs 1, 2 and 4 on their own batches (persistent queue, kernel time by the
+    session's CUDA events; warm-up run first), with parity spot checks."""
+    from gbskernels_b200 import configs, workloads
+    out = {}
+    flops = workloads.ref_flops
+    jobs = []
+    # config 1: 4096 real symmetric 16 x 16 hafnians
+    c1 = list(workloads.haf_real_batch(4096, 16, seed=1))
+    f1 = 4096 * flops("haf", 16)              # the reference evaluates real input as complex
+    f1r = 4096 * flops("haf", 16, real=True)  # the same walk in real arithmetic
+    r, v, a, st = configs.run("haf", c1, "fp64", reps=3)
+    rc, vc, ac, stc = configs.run("haf", c1, "certified", reps=2)
+    out["config1_haf16_real"] = {
+        "batch": 4096, "value": r["instances_per_s"], "unit": "instances/s", "kernel_ms": r["kernel_ms"],
+        "roofline_frac": f1 / (r["kernel_ms"] * 1e-3) / 1e12 / peak,
+        "roofline_frac_real_flops": f1r / (r["kernel_ms"] * 1e-3) / 1e12 / peak,
+        "certified": {"value": rc["instances_per_s"], "rel_bound_median": rc["rel_bound_median"],
+                      "values_equal_fp64": bool(np.array_equal(vc, v))}}
+    jobs += [("c1", i, "haf", c1[i].astype(np.complex128), v[i], ac[i]) for i in range(4)]
+    # config 2: 1024 Haar 20 x 20 permanents
+    c2 = list(workloads.perm_haar_batch(1024, 20, seed=2))
+    f2 = 1024 * flops("perm", 20)
+    r, v2, _, _ = configs.run("perm", c2, "fp64", reps=3)
+    rd, vd, _, _ = configs.run("perm", c2, "dd", reps=1)
+    out["config2_perm20"] = {
+        "batch": 1024, "value": r["instances_per_s"], "unit": "instances/s", "kernel_ms": r["kernel_ms"],
+        "roofline_frac": f2 / (r["kernel_ms"] * 1e-3) / 1e12 / peak,
+        "dd": {"value": rd["instances_per_s"], "kernel_ms": rd["kernel_ms"]}}
+    jobs += [("c2", i, "perm", c2[i], v2[i], vd[i]) for i in range(2)]
+    # config 4: 8192 threshold torontonians, 10..24 modes
+    c4 = workloads.tor_click_batch(8192, seed=4)
+    f4 = sum(flops("tor", m.shape[0]) for m in c4)
+    r, v4, _, st4 = configs.run("tor", c4, "fp64", reps=2)
+    rc4, vc4, ac4, stc4 = configs.run("tor", c4, "certified", reps=1)
+    out["config4_tor_k10to24"] = {
+        "batch": 8192, "value": r["instances_per_s"], "unit": "instances/s", "kernel_ms": r["kernel_ms"],
+        "roofline_frac": f4 / (r["kernel_ms"] * 1e-3) / 1e12 / peak, "status_ok": int((st4 == 0).sum()),
+        "certified": {"value": rc4["instances_per_s"], "rel_bound_median": rc4["rel_bound_median"],
+                      "values_equal_fp64": bool(np.array_equal(vc4, v4))}}
+    small = [i for i, m in enumerate(c4) if m.shape[0] <= 28][:4]
+    jobs += [("c4", i, "tor", c4[i], v4[i], ac4[i]) for i in small]
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(min(cores, len(jobs))) as pool:
+        truth = pool.map(_cfg_task, [(k, m) for _, _, k, m, _, _ in jobs], chunksize=1)
+    checks = {"config1_haf16_real": [], "config2_perm20": [], "config4_tor_k10to24": []}
+    keyof = {"c1": "config1_haf16_real", "c2": "config2_perm20", "c4": "config4_tor_k10to24"}
+    for (c, i, kind, m, val, extra), t in zip(jobs, truth):
+        e = {"rel_err": abs(val - t) / abs(t)}
+        if c in ("c1", "c4"):
+            e["certified_encloses"] = bool(abs(val - t) <= extra)  # extra = certified bound
+        else:
+            e["dd_rel_err"] = abs(extra - t) / abs(t)
+        checks[keyof[c]].append(e)
+    for k, lst in checks.items():
+        out[k]["check_vs_binary128_oracle"] = {
+            "instances": len(lst), "max_rel_err": float(max(x["rel_err"] for x in lst)),
+            "certified_enclose": all(x.get("certified_encloses", True) for x in lst),
+            "max_dd_rel_err": max((float(x["dd_rel_err"]) for x in lst if "dd_rel_err" in x), default=None)}
+    return out
+
 # ---------------------------------------------------------------- our implementation
 def main():
     a = _args()
@@ -308,16 +498,11 @@ def main():
     _lib.check(lib.gbs_probe_fp64_peak(_lib.dptr(tf), ctypes.byref(pms)), "gbs_probe_fp64_peak")
     peak = float(tf[0])
 
-    # ---- parity spot check on this run's own results (cheap sizes vs the oracle)
+    # ---- parity spot check on this run's own results: one haf + one lhaf per size
+    # class 8..28 against the oracle (the checker; nothing timed depends on it)
     check = {"finite": bool(np.all(np.isfinite(out))), "status_ok": bool(np.all(st == 0))}
-    if dist.rank == 0:
-        import oracle
-        errs = []
-        for i in range(B):
-            if mats[i].shape[0] <= 12 and len(errs) < 24:
-                ref = getattr(oracle, funcs[i])(mats[i], "quad")
-                errs.append(abs(out[i] - ref) / abs(ref))
-        check["max_rel_err_vs_binary128_oracle_N<=12"] = float(max(errs)) if errs else None
+    if dist.rank == 0 and not a.profile_small:
+        check.update(parity_check(funcs, mats, out, len(os.sched_getaffinity(0))))
 
     line = {"metric": METRIC, "value": value, "unit": "instances/s", "n_gpus": dist.world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * step_s,
@@ -384,6 +569,36 @@ def main():
                        "path": "gbskernels_b200.Workspace.evaluate (numpy in, numpy out)",
                        "equal_to_resident_run": bool(np.array_equal(r, out))}
 
+    # ---- the reference's plain per-size path, end to end from numpy (one synchronous
+    # session call per (function, size) bucket), against the e2e line above
+    if not a.no_per_size and not a.no_e2e:
+        with G.Workspace() as ws2:
+            per_size_sync(lib, ws2._session, funcs, mats)  # warm
+            k4 = max(1, min(a.steps, 3))
+            dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(k4):
+                r4 = per_size_sync(lib, ws2._session, funcs, mats)
+            torch.cuda.synchronize()
+            t4 = dist.max(time.perf_counter() - t0)
+        v4 = dist.world * B * k4 / t4
+        line["plain_per_size_sync"] = {
+            "value": v4, "unit": "instances/s", "ms_per_step": 1e3 * t4 / k4,
+            "buckets": len({(f, m.shape[0]) for f, m in zip(funcs, mats)}),
+            "path": "per (function, size) bucket: np.stack, gbs_session_evaluate (H2D, launch, D2H, sync), "
+                    "host scatter -- gbskernels/__init__.py:813-852 over core/host_api.cu:537-590",
+            "e2e_persistent_speedup": line["e2e"]["value"] / v4,
+            "values_equal": bool(np.array_equal(r4, out))}
+
+    # ---- batch-size sweep: where one launch per size underfills the GPU
+    if not a.no_sweep and dist.world == 1:
+        line["batch_sweep"] = batch_sweep(G, lib, (256, 1024, 4096, 16384), a.seed, stream, sptr)
+
+    # ---- the other configurations (own batches)
+    if not a.no_configs and dist.world == 1:
+        line["configs"] = other_configs(G, peak, len(os.sched_getaffinity(0)))
+
     # ---- CPU baseline (rank 0, one GPU)
     if not a.no_cpu_baseline and dist.world == 1:
         cores = len(os.sched_getaffinity(0))
@@ -394,9 +609,13 @@ def main():
                                           "trace) one process per core; rate = cores / mean per-instance "
                                           f"time ({det['cpu_seconds']:.1f} CPU-s)"}
 
-    # ---- serving loop: p50 / p99 latency beside throughput
-    if not a.no_serving and hasattr(G, "serve_stream") and dist.world == 1:
-        line["serving"] = G.serve_stream(rate=None, rate_frac=0.75, n_req=2000, seed=5)
+    # ---- serving loop: chain-rule queries on resident states, p50 / p99 latency
+    # beside throughput, below and above the offline rate
+    if not a.no_serving and dist.world == 1:
+        from gbskernels_b200.serving import offline_rate, serve_stream
+        off = offline_rate(2000, 5)
+        line["serving"] = serve_stream(rate=None, rate_frac=0.75, n_req=2000, seed=5, offline=off)
+        line["serving_saturated"] = serve_stream(rate=None, rate_frac=3.0, n_req=2000, seed=5, offline=off)
 
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
