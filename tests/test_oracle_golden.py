@@ -126,3 +126,29 @@ def test_reference_shim_kernels_match_oracle(orc, golden, func):
         vals = orc.ref_batched(func, stack, "fp64")
         for v, (m, truth) in zip(vals, cases):
             assert abs(v - getattr(orc, func)(m)) <= 1e-11 * max(abs(truth), 1.0)
+
+
+# ---------------------------------------------------------------- config-size fixture
+def test_config_fixture_truths_are_consistent():
+    """tests/golden/config_sizes.npz: the binary128 torontonians at 18..24 modes lie
+    inside the reference's own certified double-double enclosures (compiled from the
+    reference's sources), and the binary64 oracle port stays within its error scale
+    N u kappa of the binary128 hafnians and loop hafnians at N = 22..28."""
+    from pathlib import Path
+    import oracle
+    F = dict(np.load(Path(__file__).resolve().parent / "golden" / "config_sizes.npz"))
+
+    def t(q):
+        return complex(q[0] + q[1], q[2] + q[3])
+
+    for i, d in enumerate(F["c4_dims"]):
+        q = t(F["c4_quad"][i]).real
+        assert abs(q - F["c4_ref_value"][i]) <= F["c4_ref_bound"][i] * (1 + 1e-9), (d, q, F["c4_ref_value"][i])
+        assert F["c4_ref_bound"][i] <= 1e-11 * abs(q)  # a tight enclosure, not a vacuous one
+    for i, f in enumerate(F["c3_funcs"]):
+        d = int(F["c3_dims"][i])
+        m = F["c3_mats"][i, :d, :d]
+        q = t(F["c3_quad"][i])
+        v = getattr(oracle, str(f))(m, "fp64")
+        kappa = F["c3_absnorm"][i] / abs(q)
+        assert abs(v - q) / abs(q) <= 8 * d * 2.0 ** -53 * kappa, (f, d)
