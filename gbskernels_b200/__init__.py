@@ -116,140 +116,97 @@ def _call_uniform(func: str, stack: np.ndarray, precision: str) -> np.ndarray:
     return out
 
 
-def _call_aux(func: str, stack: np.ndarray, kind: str) -> tuple[np.ndarray, np.ndarray]:
-    lib = _lib.load()
-    B, d = stack.shape[0], stack.shape[1]
-    out = np.empty(B, dtype=np.complex128)
-    aux = np.empty(B, dtype=np.float64)
-    if B == 0:
-        return out, aux
-    name = f"gbs_{func}_{kind}_host"
-    fn = getattr(lib, name, None)
-    if fn is None:
-        raise NotImplementedError(f"libgbs_b200 has no {name}")
-    rc = fn(_lib.dptr(stack.view(np.float64)), _kernel_dim(func, d), B, _lib.dptr(out.view(np.float64)),
-            _lib.dptr(aux))
-    _lib.check(rc, name)
-    return out, aux
-
-
 # ------------------------------------------------------------------ tiers
+_NOT_SUPPORTED = 801  # cudaErrorNotSupported: a (function, tier) the kernels refuse
+
+
+def _raise_for(rc: int, what: str, invalid=ValueError, unsupported=ValueError) -> None:
+    """Map a library return code to the exception the API contract names: bad
+    arguments (code 1) and refused combinations (code 801) become `invalid` /
+    `unsupported`, anything else (a CUDA failure) RuntimeError."""
+    if rc == 0:
+        return
+    msg = _lib.last_error()
+    if rc == 1:
+        raise invalid(f"{what}: {msg}")
+    if rc == _NOT_SUPPORTED:
+        raise unsupported(f"{what}: {msg}")
+    raise RuntimeError(f"{what} failed (code {rc}): {msg}")
+
+
 def _auto_batched(func: str, matrices, return_diagnostics: bool):
+    """fp64 + cancellation indicator, double-double rerun of the elements with
+    kappa >= 1e8 -- one library call (gbs_auto_host)."""
     stack = _prepare(func, matrices, "fp64")
-    lib = _lib.load()
     B, d = stack.shape[0], stack.shape[1]
     out = np.empty(B, dtype=np.complex128)
     kappa = np.empty(B, dtype=np.float64)
-    tier = np.empty(B, dtype=np.int32)
-    if B and _is_complex_tor(func, stack):
-        # complex O: the indicator pass runs (subset LU), but the double-double rerun
-        # is real-domain only -- refuse like the reference's GPU dd torontonian
-        out, kappa = _call_aux(func, stack, "kappa")
-        kappa = kappa / np.maximum(np.abs(out), 1e-300)
-        if np.any(kappa >= _AUTO_KAPPA_MAX):
-            raise ValueError("precision='auto' would rerun a complex torontonian in double-double, "
-                             "which is real-domain only; use precision='fp64'")
-        tier[:] = 0
-    elif B:
-        rc = lib.gbs_auto_host(_FN[func], _lib.dptr(stack.view(np.float64)), d, B, _AUTO_KAPPA_MAX,
-                               _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier))
-        _lib.check(rc, "gbs_auto_host")
+    tier = np.zeros(B, dtype=np.int32)
+    if B:
+        rc = _lib.load().gbs_auto_host(_FN[func], _lib.dptr(stack.view(np.float64)), d, B, _AUTO_KAPPA_MAX,
+                                       _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier))
+        # a complex torontonian whose indicator asks for the (real-domain) dd rerun
+        _raise_for(rc, f"precision='auto' {func}")
     if not return_diagnostics:
         return out
-    diags = [{"tier": "dd" if t else "fp64", "cancellation": float(k)} for t, k in zip(tier, kappa)]
-    return out, diags
-
-
-def _finite_certificate(value: complex, bound: float) -> bool:
-    return (np.isfinite(value.real) and np.isfinite(value.imag) and np.isfinite(bound) and bound >= 0.0)
-
-
-def _certificate_rel(value: complex, bound: float) -> float:
-    if not _finite_certificate(value, bound):
-        return float("inf")
-    mag = abs(value)
-    if mag == 0.0:
-        return 0.0 if bound == 0.0 else float("inf")
-    return float(bound / mag)
-
-
-def _check_certified_input(A: Any) -> None:
-    try:
-        finite = np.all(np.isfinite(np.asarray(A)))
-    except (TypeError, ValueError):
-        finite = False
-    if not finite:
-        raise ValueError("certified evaluation requires finite input entries")
+    return out, [{"tier": ("fp64", "dd")[t], "cancellation": float(k)} for t, k in zip(tier, kappa)]
 
 
 def _certified_batched(func: str, matrices, rtol: float | None):
-    """Certified tier with the proven ladder certified-fp64 -> certified-dd
-    (gbskernels/__init__.py:374-478; the mpmath rung is CPU-only and not here:
-    an element that neither rung certifies to rtol raises FloatingPointError)."""
+    """Certified values and bounds; with `rtol`, the proven ladder certified-fp64 ->
+    certified-dd runs inside the library (gbs_certified_ladder_host).  An element no
+    rung certifies raises FloatingPointError (the reference's mpmath rung is
+    CPU-only)."""
     stack = _prepare(func, matrices, "fp64")
-    _check_certified_input(stack)
-    if _is_complex_tor(func, stack):
-        raise NotImplementedError("certified torontonian is real-domain only (the bound rests on the "
-                                  "Cholesky factor of I - O_S); the input has non-zero imaginary parts")
-    values, bounds = _call_aux(func, stack, "certified")
-    out = values.astype(np.complex128, copy=True)
+    B, d = stack.shape[0], stack.shape[1]
+    out = np.empty(B, dtype=np.complex128)
+    bound = np.empty(B, dtype=np.float64)
+    tier = np.zeros(B, dtype=np.int32)
+    if B:
+        rc = _lib.load().gbs_certified_ladder_host(_FN[func], _lib.dptr(stack.view(np.float64)), d, B,
+                                                   -1.0 if rtol is None else float(rtol),
+                                                   _lib.dptr(out.view(np.float64)), _lib.dptr(bound),
+                                                   _lib.iptr(tier))
+        _raise_for(rc, f"certified {func}", unsupported=NotImplementedError)
+    bad = np.flatnonzero(tier < 0)
+    if bad.size:
+        i = int(bad[0])
+        if rtol is None:
+            raise FloatingPointError(f"certified {func} batch element {i} refused with a non-finite value or bound")
+        raise FloatingPointError(f"certified {func} element {i}: neither the fp64 nor the double-double "
+                                 f"certificate reaches rtol={rtol} (the mpmath rung is CPU-only)")
+    mag = np.abs(out)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(mag > 0, bound / np.where(mag > 0, mag, 1.0), np.where(bound == 0, 0.0, np.inf))
     diags = []
-    redo = []
-    for i in range(len(out)):
-        v, e = complex(out[i]), float(bounds[i])
-        valid = _finite_certificate(v, e)
-        rel = _certificate_rel(v, e)
-        if rtol is not None and (not valid or not np.isfinite(rel) or rel > rtol):
-            redo.append(i)
-            diags.append(None)
-        elif not valid:
-            raise FloatingPointError(
-                f"certified {func} batch element {i} refused with a non-finite value or bound")
-        else:
-            d = {"tier": "certified-fp64", "abs_error_bound": e, "rel_error_bound": rel}
-            if rtol is not None:
-                d["escalated"] = False
-            diags.append(d)
-    if redo:
-        sub = np.ascontiguousarray(stack[redo])
-        if getattr(_lib.load(), f"gbs_{func}_dd_certified_host", None) is None:
-            raise FloatingPointError(
-                f"certified {func}: the fp64 certificate does not reach rtol={rtol} and this "
-                "build has no double-double certificate for it (the mpmath rung is CPU-only)")
-        v2, b2 = _call_aux(func, sub, "dd_certified")
-        for j, i in enumerate(redo):
-            vc, bf = complex(v2[j]), float(b2[j])
-            rel2 = _certificate_rel(vc, bf)
-            if _finite_certificate(vc, bf) and np.isfinite(rel2) and rel2 <= rtol:
-                out[i] = vc
-                diags[i] = {"tier": "certified-dd", "escalated": True, "abs_error_bound": bf,
-                            "rel_error_bound": float(rel2)}
-            else:
-                raise FloatingPointError(
-                    f"certified {func} element {i}: neither the fp64 nor the double-double "
-                    f"certificate reaches rtol={rtol} (the mpmath rung is CPU-only)")
+    for t, e, r in zip(tier, bound, rel):
+        dg = {"tier": "certified-dd" if t == _TIER["certified-dd"] else "certified-fp64",
+              "abs_error_bound": float(e), "rel_error_bound": float(r)}
+        if rtol is not None:
+            dg["escalated"] = bool(t == _TIER["certified-dd"])
+        diags.append(dg)
     return out, diags
 
 
-def _check_diag(precision, return_diagnostics):
+def _validate_options(precision, return_diagnostics, rtol) -> None:
+    """The API's option contract: diagnostics exist for the auto and certified tiers
+    only and the certified tier must return them (its bound is the point of it);
+    rtol belongs to the certified tier and is a finite non-negative number."""
     if return_diagnostics and precision not in ("auto", "certified"):
         raise ValueError("return_diagnostics=True requires precision='auto' or 'certified'")
     if precision == "certified" and not return_diagnostics:
-        raise ValueError(
-            "precision='certified' returns its error bound via diagnostics; call with "
-            "return_diagnostics=True (a certificate you cannot see is not a certificate)")
-
-
-def _check_rtol(precision, rtol):
-    if rtol is not None and precision != "certified":
-        raise ValueError("rtol is a certified-tier parameter; it requires precision='certified'")
-    if rtol is not None and (not np.isfinite(rtol) or rtol < 0.0):
+        raise ValueError("precision='certified' reports the bound of its certificate in the diagnostics: "
+                         "pass return_diagnostics=True")
+    if rtol is None:
+        return
+    if precision != "certified":
+        raise ValueError("rtol is a parameter of precision='certified'")
+    if not np.isfinite(rtol) or rtol < 0.0:
         raise ValueError("rtol must be finite and non-negative")
 
 
 def _dispatch_batched(func, matrices, precision, backend, return_diagnostics=False, rtol=None):
-    _check_diag(precision, return_diagnostics)
-    _check_rtol(precision, rtol)
+    _validate_options(precision, return_diagnostics, rtol)
     _check_backend(backend)
     if precision == "auto":
         return _auto_batched(func, matrices, return_diagnostics)
@@ -346,9 +303,6 @@ def lhaf_repeated(A: Any, gamma: Any, reps: Any, backend: str = "gpu", certified
         raise ValueError(f"lhaf_repeated: reps must be (B, {M}) or ({M},), got {np.asarray(reps).shape}")
     if (r < 0).any():
         raise ValueError("lhaf_repeated: reps must be non-negative")
-    if certified:
-        _check_certified_input(A)
-        _check_certified_input(g)
     if M > 32:
         raise ValueError(f"lhaf_repeated: M = {M} exceeds the cap 32")
     if r.size and int(r.sum(axis=1).max()) > 64:
@@ -657,29 +611,36 @@ class Workspace:
         return self._ragged("tor", matrices, precision)
 
     def _ragged(self, func: str, matrices, precision: str) -> np.ndarray:
+        """One function over a ragged batch: every size in one persistent launch (the
+        auto tier in two: fp64 + indicator, then the double-double reruns).  A
+        rejected matrix raises ValueError naming its position."""
         self._require()
+        if precision == "ref":
+            raise NotImplementedError("'ref' is the mpmath ground truth -- CPU only (backend='cpu').")
+        if precision not in ("fp64", "dd", "auto"):
+            raise ValueError(f"unknown precision {precision!r} for a ragged batch; expected fp64, dd or auto")
         mats = _as_square_list(matrices)
-        if not mats:
-            return np.empty(0, dtype=np.complex128)
-        if precision == "auto":
-            # per-element auto within uniform buckets (value identical to evaluating alone)
-            out = np.empty(len(mats), dtype=np.complex128)
-            buckets: dict[int, list[int]] = {}
-            for i, a in enumerate(mats):
-                buckets.setdefault(a.shape[0], []).append(i)
-            for d, idxs in buckets.items():
-                try:
-                    res = _auto_batched(func, np.stack([mats[i] for i in idxs]), False)
-                except ValueError as e:
-                    raise ValueError(f"matrix #{idxs[0]} (dim {d}): {e}") from e
-                out[idxs] = res
+        B = len(mats)
+        out = np.empty(B, dtype=np.complex128)
+        if B == 0:
             return out
-        for i, a in enumerate(mats):
-            try:
-                _prepare(func, a[None], precision)
-            except ValueError as e:
-                raise ValueError(f"matrix #{i} (dim {a.shape[0]}): {e}") from e
-        return self.evaluate([func] * len(mats), mats, [precision] * len(mats))
+        buf, dims, offs = _pack(mats)
+        fns = np.full(B, _FN[func], dtype=np.int32)
+        lib = _lib.load()
+        if precision == "auto":
+            kappa = np.empty(B)
+            tier = np.zeros(B, dtype=np.int32)
+            rc = lib.gbs_queue_evaluate_auto(self._session, B, _lib.iptr(fns), _lib.iptr(dims), _lib.llptr(offs),
+                                             _lib.dptr(buf.view(np.float64)), _AUTO_KAPPA_MAX,
+                                             _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier),
+                                             None)
+        else:
+            tiers = np.full(B, _TIER[precision], dtype=np.int32)
+            rc = lib.gbs_queue_evaluate(self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims),
+                                        _lib.llptr(offs), _lib.dptr(buf.view(np.float64)),
+                                        0 if self._persistent else 1, _lib.dptr(out.view(np.float64)), None, None)
+        _raise_for(rc, f"Workspace.{func}_batched")
+        return out
 
     def evaluate(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str],
                  return_status: bool = False):
@@ -731,10 +692,8 @@ class Workspace:
         if not uniform:
             raise ValueError("device-resident output of a ragged batch: use Workspace.evaluate_resident")
         stack = _prepare(func, stack, "dd" if precision == "dd" else "fp64")
-        if precision == "certified":
-            _check_certified_input(stack)
-            if _is_complex_tor(func, stack):
-                raise NotImplementedError("certified torontonian is real-domain only")
+        if precision == "certified" and _is_complex_tor(func, stack):
+            raise NotImplementedError("certified torontonian is real-domain only")
         if precision == "auto" and _is_complex_tor(func, stack):
             raise NotImplementedError("auto torontonian of a complex O: the double-double rerun is "
                                       "real-domain only; use precision='fp64'")
@@ -744,7 +703,7 @@ class Workspace:
         rc = _lib.load().gbs_session_evaluate_resident_tier(self._session, _FN[func], tier,
                                                             _lib.dptr(stack.view(np.float64)), d, B,
                                                             ctypes.byref(ptr))
-        _lib.check(rc, "gbs_session_evaluate_resident_tier")
+        _raise_for(rc, f"Workspace.{func}_resident", unsupported=NotImplementedError)
         return _ResidentResult(ptr, B)
 
     def evaluate_resident(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str] | None = None):

@@ -36,6 +36,10 @@ SIGNATURES: dict[str, tuple[list, object]] = {
        for f in ("perm", "haf", "lhaf", "tor")},
     "gbs_auto_host": ([ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _ip],
                       ctypes.c_int),
+    "gbs_certified_ladder_host": ([ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _ip],
+                                  ctypes.c_int),
+    "gbs_queue_evaluate_auto": ([_vp, ctypes.c_int, _ip, _ip, _llp, _dp, ctypes.c_double, _dp, _dp, _ip, _ip],
+                                ctypes.c_int),
     # single-large torontonian
     "gbs_tor_recursive_single_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
     "gbs_tor_single_certified_host": ([_dp, ctypes.c_int, ctypes.c_int, _dp, _dp], ctypes.c_int),

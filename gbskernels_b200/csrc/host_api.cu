@@ -1179,6 +1179,52 @@ int gbs_auto_host(int func, const double* m, int dim, int b, double kappa_max, d
   return rc;
 }
 
+// ---- certified tier with the proven rtol ladder (gbskernels/__init__.py:374-478) ----
+// The binary64 certificate first; every element whose bound does not prove a
+// relative error <= rtol (or is not finite) is re-evaluated by the certified
+// double-double rung in one more launch.  tier_out[i]: 3 certified binary64,
+// 4 certified double-double, -1 no rung certifies it.  rtol < 0: no ladder (the
+// binary64 certificate as it is; -1 where it is not finite).  The reference's last
+// rung (mpmath on the host) has no counterpart: a refused element stays refused.
+static bool certificate_meets(double re, double im, double e, double rtol) {
+  if (!(std::isfinite(re) && std::isfinite(im) && std::isfinite(e) && e >= 0.0)) return false;
+  if (rtol < 0.0) return true;
+  const double mag = std::hypot(re, im);
+  if (mag == 0.0) return e == 0.0;
+  return e / mag <= rtol;
+}
+
+int gbs_certified_ladder_host(int func, const double* m, int dim, int b, double rtol, double* o, double* bound,
+                              int* tier_out) {
+  if (b <= 0) return 0;
+  if (!m || !o || !bound || !tier_out) return fail(cudaErrorInvalidValue, "null buffer");
+  if (func < kFnPerm || func > kFnTor) return fail(cudaErrorInvalidValue, "unknown function code");
+  if (func == kFnTor && (dim & 1)) return fail(cudaErrorInvalidValue, "torontonian: matrix side must be even");
+  int rc = one_shot_cert(func, m, dim, b, o, bound, kTierCert);
+  if (rc) return rc;
+  std::vector<int> redo;
+  for (int i = 0; i < b; ++i) {
+    const bool ok = certificate_meets(o[2 * i], o[2 * i + 1], bound[i], rtol);
+    tier_out[i] = ok ? kTierCert : -1;
+    if (!ok && rtol >= 0.0) redo.push_back(i);
+  }
+  if (redo.empty()) return 0;
+  const size_t nn = 2ull * (size_t)dim * dim;
+  std::vector<double> sub(nn * redo.size()), o2(2 * redo.size()), b2(redo.size());
+  for (size_t j = 0; j < redo.size(); ++j) std::memcpy(&sub[j * nn], m + redo[j] * nn, nn * sizeof(double));
+  rc = one_shot_cert(func, sub.data(), dim, (int)redo.size(), o2.data(), b2.data(), kTierCertDD);
+  if (rc) return rc;
+  for (size_t j = 0; j < redo.size(); ++j) {
+    if (!certificate_meets(o2[2 * j], o2[2 * j + 1], b2[j], rtol)) continue;
+    const int i = redo[j];
+    o[2 * i] = o2[2 * j];
+    o[2 * i + 1] = o2[2 * j + 1];
+    bound[i] = b2[j];
+    tier_out[i] = kTierCertDD;
+  }
+  return 0;
+}
+
 // ---- sessions (core/host_api.cu:521-658) --------------------------------------
 int gbs_session_open(gbs_session** out) {
   if (!out) return fail(cudaErrorInvalidValue, "null session pointer");
@@ -1284,6 +1330,27 @@ int gbs_queue_evaluate(gbs_session* s, int B, const int* funcs, const int* tiers
   opt.per_size = (mode == 1);
   std::lock_guard<std::mutex> lk(s->mu);
   int rc = run_batch(s, reqs, out, aux, st.data(), opt);
+  if (rc) return rc;
+  if (status) std::memcpy(status, st.data(), sizeof(int) * B);
+  apply_status(B, out, st.data());
+  return 0;
+}
+
+// Ragged / mixed batch in the auto tier: every request's fp64 value with its
+// indicator in one launch, then the requests with kappa >= kappa_max rerun in
+// double-double in one more (gbskernels/__init__.py:272-297 per element, without
+// the reference's per-size buckets).  tier_out[i]: 0 fp64 kept, 1 dd rerun.
+int gbs_queue_evaluate_auto(gbs_session* s, int B, const int* funcs, const int* dims, const long long* offsets,
+                            const double* mats, double kappa_max, double* out, double* kappa, int* tier_out,
+                            int* status) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  if (B <= 0) return 0;
+  if (!funcs || !dims || !offsets || !mats || !out || !tier_out) return fail(cudaErrorInvalidValue, "null buffer");
+  std::vector<Req> reqs(B);
+  for (int i = 0; i < B; ++i) reqs[i] = Req{funcs[i], kTierFp64, dims[i], mats + 2 * offsets[i]};
+  std::vector<int> st(B);
+  std::lock_guard<std::mutex> lk(s->mu);
+  const int rc = auto_batch(s, reqs, kappa_max, out, kappa, tier_out, st.data());
   if (rc) return rc;
   if (status) std::memcpy(status, st.data(), sizeof(int) * B);
   apply_status(B, out, st.data());

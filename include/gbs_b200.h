@@ -139,6 +139,20 @@ const char* gbs_sampler_last_error(void);
 int gbs_auto_host(int func, const double* mats, int dim, int batch, double kappa_max, double* out,
                   double* kappa, int* tier_out);
 
+/* ---- certified tier with the rtol ladder --------------------------------------
+ * reference: the certified ladder of gbskernels/__init__.py:374-478 (_certified_single
+ * / _certified_batched), whose GPU rungs are gbs_*_certified_host and
+ * gbs_*_dd_certified_host; here the whole ladder is one call.  func: 0 perm, 1 haf,
+ * 2 lhaf, 3 tor; dim = matrix side (tor: 2n).  The binary64 certificate first;
+ * elements whose bound does not prove |error| / |value| <= rtol, or is not finite,
+ * are re-evaluated by the certified double-double rung.  tier_out[i]: 3 certified
+ * binary64, 4 certified double-double, -1 neither rung certifies it (the
+ * reference's mpmath rung is CPU-only and has no counterpart).  rtol < 0: no
+ * ladder (-1 marks a non-finite binary64 certificate).  Non-finite input returns
+ * cudaErrorInvalidValue; a complex torontonian cudaErrorNotSupported.            */
+int gbs_certified_ladder_host(int func, const double* mats, int dim, int batch, double rtol, double* out,
+                              double* bound, int* tier_out);
+
 /* ---- resident sessions -------------------------------------------------------
  * reference: core/host_api.cu:521-658 (gbs_session_open ... gbs_dev_free)
  * func: 0 perm, 1 haf, 2 lhaf, 3 tor; prec: 0 fp64, 1 dd.  dim = matrix side.  */
@@ -184,6 +198,13 @@ int gbs_dev_device(const void* d, int* device);
 int gbs_queue_evaluate(gbs_session* s, int batch, const int* funcs, const int* tiers, const int* dims,
                        const long long* offsets, const double* mats, int mode, double* out, double* aux,
                        int* status);
+/* auto tier over a ragged / mixed batch (tiers are implied): fp64 + indicator for
+ * every request in one launch, kappa >= kappa_max reruns in double-double in one
+ * more; tier_out[i] 0 fp64, 1 dd; kappa[i] = sum|term| / |value|.
+ * reference: gbskernels/__init__.py:799-812 (Workspace auto, per size bucket).    */
+int gbs_queue_evaluate_auto(gbs_session* s, int batch, const int* funcs, const int* dims, const long long* offsets,
+                            const double* mats, double kappa_max, double* out, double* kappa, int* tier_out,
+                            int* status);
 /* device-resident plan: validate, cut and upload once; run many times on `stream`
  * (a cudaStream_t, or NULL for the session stream); read results back.  Used for
  * timing with inputs resident in HBM and by servers that re-run a fixed batch.   */

@@ -339,3 +339,56 @@ def test_tor_complex_contract(gpu):
         together = ws.tor_batched(mats)
     alone = np.array([gpu.tor_batched(m[None])[0] for m in mats])
     assert np.array_equal(together, alone)
+
+
+def test_ragged_auto_equals_each_element_alone(gpu):
+    """Workspace auto over a ragged batch (gbs_queue_evaluate_auto: one fp64 +
+    indicator launch over every size, one double-double launch of the reruns) gives
+    each element the value the uniform auto tier gives it alone."""
+    g = np.random.default_rng(9)
+    delta = 1e-9
+    Bk = np.array([[0, 1, 1, 1], [1, 0, delta - 2, 1], [1, delta - 2, 0, 1], [1, 1, 1, 0]], dtype=complex)
+    G2 = g.standard_normal((4, 4))
+    R = G2 + G2.T
+    np.fill_diagonal(R, 0)
+    A = np.zeros((8, 8), dtype=complex)
+    A[:4, :4], A[4:, 4:] = Bk, R  # cancels: rerun in double-double
+    mats = [sym(6), A, sym(12), sym(6), A.copy(), sym(10)]
+    with gpu.Workspace() as ws:
+        rag = ws.haf_batched(mats, precision="auto")
+    for i, m in enumerate(mats):
+        v, d = gpu.haf(m, precision="auto", return_diagnostics=True)
+        assert rag[i] == v, i
+        assert d["tier"] == ("dd" if m.shape[0] == 8 else "fp64")
+
+
+def test_certified_ladder_in_library(gpu, lib, orc):
+    """gbs_certified_ladder_host: an rtol the binary64 certificate meets keeps it
+    (tier 3); a tighter one escalates to the certified double-double rung (tier 4,
+    its bound still enclosing the binary128 truth); one that no rung meets is
+    refused (tier -1)."""
+    import ctypes
+    mats = np.stack([sym(12) for _ in range(3)])
+    truth = [orc.haf(m, "quad") for m in mats]
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+
+    def ladder(rtol):
+        out = np.empty(3, np.complex128)
+        bnd = np.empty(3)
+        tier = np.zeros(3, np.int32)
+        rc = lib.gbs_certified_ladder_host(1, mats.ctypes.data_as(dp), 12, 3, rtol, out.ctypes.data_as(dp),
+                                           bnd.ctypes.data_as(dp), tier.ctypes.data_as(ip))
+        assert rc == 0
+        return out, bnd, tier
+
+    for rtol, want in ((1e-3, 3), (1e-14, 4), (1e-30, -1)):
+        out, bnd, tier = ladder(rtol)
+        assert list(tier) == [want] * 3, (rtol, tier, bnd / np.abs(out))
+        if want > 0:
+            for i in range(3):
+                assert abs(out[i] - truth[i]) <= bnd[i] * (1 + 1e-12) + 1e-300
+    v, d = gpu.haf_batched(mats, precision="certified", return_diagnostics=True, rtol=1e-14)
+    assert all(x["escalated"] and x["tier"] == "certified-dd" for x in d)
+    with pytest.raises(FloatingPointError, match="rtol"):
+        gpu.haf_batched(mats, precision="certified", return_diagnostics=True, rtol=1e-30)
