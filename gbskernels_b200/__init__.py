@@ -692,8 +692,6 @@ class Workspace:
         if not uniform:
             raise ValueError("device-resident output of a ragged batch: use Workspace.evaluate_resident")
         stack = _prepare(func, stack, "dd" if precision == "dd" else "fp64")
-        if precision == "certified" and _is_complex_tor(func, stack):
-            raise NotImplementedError("certified torontonian is real-domain only")
         if precision == "auto" and _is_complex_tor(func, stack):
             raise NotImplementedError("auto torontonian of a complex O: the double-double rerun is "
                                       "real-domain only; use precision='fp64'")

@@ -182,20 +182,24 @@ __device__ ItemResult tor_item(const double* __restrict__ mats, const InstDesc& 
   const double* Oc = mats + d.off;
   if (!d.real_in) {
     // complex O (binary64 tiers only; the host refuses the others): one warp per
-    // subset LU, w.count masks from w.lo (tor_lu.cuh)
-    if constexpr (TIER == kTierFp64 || TIER == kTierKappa) {
-      cplx acc = mkc(0.0, 0.0);
+    // subset LU, w.count masks from w.lo (tor_lu.cuh); the certified tier carries
+    // ball radii through the same LU (value = the fp64 value bit for bit)
+    if constexpr (TIER == kTierFp64 || TIER == kTierKappa || TIER == kTierCert) {
+      constexpr bool CERT = TIER == kTierCert;
+      cball acc{mkc(0.0, 0.0), 0.0};
       double aabs = 0.0;
       bool sing = false;
       for (unsigned long long k = 0; k < w.count; ++k) {
-        const cplx t = tor_lu_term(Oc, n, (uint32_t)(w.lo + k), ws, lane, sing);
-        acc = cadd(acc, t);
-        if (TIER == kTierKappa) aabs += hypot(t.re, t.im);
+        const cball t = tor_lu_term<CERT>(Oc, n, (uint32_t)(w.lo + k), ws, lane, sing);
+        if constexpr (CERT) acc = cb_add(acc, t);
+        else acc.z = cadd(acc.z, t.z);
+        if (TIER == kTierKappa) aabs += hypot(t.z.re, t.z.im);
         __syncwarp();
       }
-      r.val = ddc_from_c(acc);
-      r.aux = aabs;
-      if (sing) r.st = kStOffDomain;
+      r.val = ddc_from_c(acc.z);
+      r.aux = CERT ? acc.r : aabs;
+      if (sing) r.st = CERT ? kStUncertified : kStOffDomain;
+      else if (CERT && !(acc.r < INFINITY)) r.st = kStUncertified;
     } else {
       r.st = kStTooLarge;
     }

@@ -267,7 +267,7 @@ static int ws_for_plan(const Plan& P) {
     const int fn = ft_fn(d.ft), tier = ft_tier(d.ft);
     int w = 0;
     if (fn == kFnPerm) w = 2 * d.dim * d.dim;
-    else if (fn == kFnTor && !d.real_in) w = tor_lu_ws_doubles();
+    else if (fn == kFnTor && !d.real_in) w = tor_lu_ws_doubles(tier == kTierCert);
     else if (fn == kFnTor && (tier == kTierDD || tier == kTierCertDD)) w = tor_d_layout(d.dim / 2, tier == kTierCertDD).total;
     else if (fn == kFnTor) w = tor_w_layout(d.dim / 2, tier == kTierCert).total;
     else if (tier == kTierDD || tier == kTierCertDD) w = haf_dd_layout(P.haf_smax, tier == kTierCertDD).total;
@@ -410,10 +410,10 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
       }
       if (!re) {
         // complex O: subset LU determinants, binary64 tiers, the reference's GPU cap
-        if (r.tier == kTierDD || r.tier == kTierCert || r.tier == kTierCertDD || r.single)
+        if (r.tier == kTierDD || r.tier == kTierCertDD || r.single)
           return fail(cudaErrorNotSupported,
-                      "torontonian: complex O is supported in the fp64 tier only (the double-double, "
-                      "certified and single-large paths are real-domain)");
+                      "torontonian: complex O is supported in the binary64 tiers only (the double-double "
+                      "and single-large paths are real-domain)");
         if (r.dim / 2 > kTorLuMaxModes)
           return fail(cudaErrorInvalidValue, "torontonian: complex O above the cap of 12 modes");
         *real_in = false;
@@ -1202,14 +1202,17 @@ int gbs_certified_ladder_host(int func, const double* m, int dim, int b, double 
   if (func == kFnTor && (dim & 1)) return fail(cudaErrorInvalidValue, "torontonian: matrix side must be even");
   int rc = one_shot_cert(func, m, dim, b, o, bound, kTierCert);
   if (rc) return rc;
+  const size_t nn = 2ull * (size_t)dim * dim;
   std::vector<int> redo;
   for (int i = 0; i < b; ++i) {
     const bool ok = certificate_meets(o[2 * i], o[2 * i + 1], bound[i], rtol);
     tier_out[i] = ok ? kTierCert : -1;
-    if (!ok && rtol >= 0.0) redo.push_back(i);
+    bool real = true;  // the double-double torontonian is real-domain only
+    if (func == kFnTor)
+      for (size_t k = 1; k < nn && real; k += 2) real = m[i * nn + k] == 0.0;
+    if (!ok && rtol >= 0.0 && real) redo.push_back(i);
   }
   if (redo.empty()) return 0;
-  const size_t nn = 2ull * (size_t)dim * dim;
   std::vector<double> sub(nn * redo.size()), o2(2 * redo.size()), b2(redo.size());
   for (size_t j = 0; j < redo.size(); ++j) std::memcpy(&sub[j * nn], m + redo[j] * nn, nn * sizeof(double));
   rc = one_shot_cert(func, sub.data(), dim, (int)redo.size(), o2.data(), b2.data(), kTierCertDD);

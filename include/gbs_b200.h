@@ -149,7 +149,8 @@ int gbs_auto_host(int func, const double* mats, int dim, int batch, double kappa
  * binary64, 4 certified double-double, -1 neither rung certifies it (the
  * reference's mpmath rung is CPU-only and has no counterpart).  rtol < 0: no
  * ladder (-1 marks a non-finite binary64 certificate).  Non-finite input returns
- * cudaErrorInvalidValue; a complex torontonian cudaErrorNotSupported.            */
+ * cudaErrorInvalidValue.  A complex torontonian has the binary64 rung only (its
+ * certificate comes from ball arithmetic through the subset LU).                 */
 int gbs_certified_ladder_host(int func, const double* mats, int dim, int batch, double rtol, double* out,
                               double* bound, int* tier_out);
 

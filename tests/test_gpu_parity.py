@@ -326,12 +326,28 @@ def test_tor_complex_vs_binary128_oracle(gpu, orc, n):
                 gpu.tor_batched(mats[i:i + 1], precision="auto")
 
 
+@pytest.mark.parametrize("n", [1, 3, 6, 9])
+def test_tor_complex_certified_encloses(gpu, orc, n):
+    """Certified tier for a complex O: ball arithmetic through the same subset LU
+    (value = the fp64 value bit for bit), the radius enclosing the binary128 LU
+    torontonian; there is no double-double rung for a complex O, so an rtol below
+    the binary64 certificate is refused."""
+    mats = np.stack([complex_O(n) for _ in range(3)])
+    fp = gpu.tor_batched(mats)
+    v, d = gpu.tor_batched(mats, precision="certified", return_diagnostics=True)
+    for i in range(3):
+        truth = orc.tor(mats[i], "quad")
+        assert v[i] == fp[i]
+        assert abs(v[i] - truth) <= d[i]["abs_error_bound"] * (1 + 1e-12), (n, i, d[i])
+        assert d[i]["tier"] == "certified-fp64" and np.isfinite(d[i]["abs_error_bound"])
+    with pytest.raises(FloatingPointError):
+        gpu.tor_batched(mats, precision="certified", return_diagnostics=True, rtol=1e-40)
+
+
 def test_tor_complex_contract(gpu):
     O = complex_O(4)[None]
     with pytest.raises(ValueError, match="real-domain"):
         gpu.tor_batched(O, precision="dd")
-    with pytest.raises(NotImplementedError, match="real-domain"):
-        gpu.tor_batched(O, precision="certified", return_diagnostics=True)
     with pytest.raises(ValueError, match="limit 24"):
         gpu.tor_batched(complex_O(13)[None])
     with gpu.Workspace() as ws:  # ragged mix of real and complex O in one queue
