@@ -134,11 +134,22 @@ static __device__ ddball haf_subset_term_dd(const double* __restrict__ A, int N,
     gi[lane] = 2 * (__ffs(mm) - 1) + (lane & 1);
   }
   __syncwarp();
+  bool tiny_halving = false;  // certified: a halving that may have rounded (see below)
   for (int e = lane; e < s * s; e += 32) {
     int r = e / s, c = e - r * s;
     int rr = gi[r], cc = gi[c ^ 1];
-    cplx v = (loop || rr != cc) ? ld_c(A + ((size_t)rr * N + cc) * 2) : mkc(0.0, 0.0);
-    st_ddc(Cs + e * 4, ddc_make(v));
+    ddc v = ddc_zero();
+    if (loop || rr != cc) {
+      // the symmetric part (A + A^T)/2 exactly, as a double word: TwoSum of the two
+      // entries, halved (the half-power identities need B_S symmetric)
+      const cplx x = ld_c(A + ((size_t)rr * N + cc) * 2), y = ld_c(A + ((size_t)cc * N + rr) * 2);
+      double er, ei;
+      const double sr = two_sum(x.re, y.re, er), si = two_sum(x.im, y.im, ei);
+      v = ddc{dd{0.5 * sr, 0.5 * er}, dd{0.5 * si, 0.5 * ei}};
+      if (CERT && (2.0 * v.re.lo != er || 2.0 * v.im.lo != ei || 2.0 * v.re.hi != sr || 2.0 * v.im.hi != si))
+        tiny_halving = true;
+    }
+    st_ddc(Cs + e * 4, v);
   }
   if (loop && lane < s) st_ddc(Dv + lane * 4, ddc_make(ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2)));
   for (int k = lane; k <= n; k += 32) {
@@ -160,7 +171,10 @@ static __device__ ddball haf_subset_term_dd(const double* __restrict__ A, int N,
       double a = 0.0;
       if (r < s && c < s) {
         const int rr = gi[r], cc = gi[c ^ 1];
-        if (loop || rr != cc) a = ru_abs_c(ld_c(A + ((size_t)rr * N + cc) * 2));
+        // >= |(A_rc + A_cr) / 2|, the modulus of the staged double-word entry
+        if (loop || rr != cc)
+          a = ru_mul(0.5, ru_add(ru_abs_c(ld_c(A + ((size_t)rr * N + cc) * 2)),
+                                 ru_abs_c(ld_c(A + ((size_t)cc * N + rr) * 2))));
       }
       st_c(Ca + (r * cs + c) * 2, mkc(a, 0.0));
     }
@@ -305,7 +319,7 @@ static __device__ ddball haf_subset_term_dd(const double* __restrict__ A, int N,
       bT[0] = e[n].r;
     }
     __syncwarp();
-    rad = bT[0];
+    rad = __any_sync(0xffffffffu, tiny_halving) ? INFINITY : bT[0];
   } else {
     if (lane == 0) {
       for (int k = 1; k <= n; ++k) {

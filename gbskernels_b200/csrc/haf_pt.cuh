@@ -508,6 +508,7 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   }
   __syncwarp();
   const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
+  bool tiny_halving = false;                    // certified tier: see the staging below
   // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
   const int dr = 32 / ccols, dc = 32 - dr * ccols;  // (r, c) advance per 32 elements
   int r = lane / ccols, c = lane - (lane / ccols) * ccols;
@@ -519,7 +520,22 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     cplx v = mkc(0.0, 0.0);
     if (c < s && r < s) {
       const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
-      if (loop || rr != cc) v = ld_c(A + ((size_t)rr * N + cc) * 2);
+      if (loop || rr != cc) {
+        // the symmetric part (A + A^T)/2, exact for a symmetric A: the half-power
+        // identities need B_S symmetric, and the reference's n-1 products of the
+        // raw entries agree with those of the symmetric part to second order in
+        // the antisymmetric part
+        const cplx x = ld_c(A + ((size_t)rr * N + cc) * 2), y = ld_c(A + ((size_t)cc * N + rr) * 2);
+        v = cscale(cadd(x, y), 0.5);
+        if constexpr (CERT) {
+          // halving a sum below twice the smallest normal can round absolutely: no
+          // certificate for such an entry (the relative input bound would not hold)
+          const cplx w = cadd(x, y);
+          if ((x.re != y.re || x.im != y.im) && fmin(fabs(w.re) > 0.0 ? fabs(w.re) : 1.0,
+                                                     fabs(w.im) > 0.0 ? fabs(w.im) : 1.0) < 4.450147717014403e-308)
+            tiny_halving = true;
+        }
+      }
     }
     st_c(Cs + (r * cs + c) * 2, v);
     if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
@@ -591,35 +607,42 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       // strip, then the strips (at most s + 1 sums; sqrt(2) gamma_{s+4} <= gamma_{2s+8}
       // per component pair)
       const double gv = ru_add(4.0 * kU, gamma_ru(2.0 * s + 8.0, kU));
-      double ca[kHafMaxPow + 2], ph[kHafMaxPow + 2], ka[kHafMaxPow + 2];
-      ca[0] = 0.0; ph[0] = 1.0; ca[1] = 0.0; ph[1] = 1.0;
+      // Input error: the staged C^ is the rounded symmetric part, |C - C^| <= c1 |C^|
+      // with c1 = u/(1-u) (exactly 0 for a symmetric A; charged regardless), so
+      // |C^a| <= t_a M_a with t_a = (1 + c1)^a, and the power errors E_a <= c_a M_a
+      // follow c_1 = c1, c_{a+1} = c_a + c1 t_a + sqrt2 gamma_2s (t_a + c_a).
+      const double c1 = kUc;
+      double ca[kHafMaxPow + 2], ph[kHafMaxPow + 2], ka[kHafMaxPow + 2], ta[kHafMaxPow + 2];
+      ca[0] = 0.0; ph[0] = 1.0; ca[1] = c1; ph[1] = 1.0; ta[0] = 1.0; ta[1] = ru_add(1.0, c1);
       for (int a = 1; a <= h; ++a) {
-        ca[a + 1] = ru_add(ca[a], ru_mul(ru_mul(sq2, g2s), ru_add(1.0, ca[a])));
+        ca[a + 1] = ru_add(ru_add(ca[a], ru_mul(c1, ta[a])), ru_mul(ru_mul(sq2, g2s), ru_add(ta[a], ca[a])));
         ph[a + 1] = ru_div(ph[a], rd_sub(1.0, g2s));
+        ta[a + 1] = ru_mul(ta[a], ru_add(1.0, c1));
       }
       ka[0] = 0.0;
-      for (int a = 1; a <= h; ++a) ka[a] = ru_add(ca[a], ru_mul(gy, ru_add(1.0, ca[a])));
+      for (int a = 1; a <= h; ++a) ka[a] = ru_add(ca[a], ru_mul(gy, ru_add(ta[a], ca[a])));
       cball kgb[kHafMaxPairs + 1];
       for (int k = 1; k <= n; ++k) {
         double ep;
         if (k == 1) {
-          ep = ru_mul(gamma_ru(6.0, kU), bT[1]);
+          ep = ru_mul(ru_add(gamma_ru(6.0, kU), c1), bT[1]);
         } else if ((k & 1) == 0) {
           const int a = k / 2;
-          double f = ru_add(ru_add(ru_mul(2.0, ca[a]), ru_mul(ca[a], ca[a])),
-                            ru_mul(g64, ru_mul(ru_add(1.0, ca[a]), ru_add(1.0, ca[a]))));
+          double f = ru_add(ru_mul(ca[a], ru_add(ru_mul(2.0, ta[a]), ca[a])),
+                            ru_mul(g64, ru_mul(ru_add(ta[a], ca[a]), ru_add(ta[a], ca[a]))));
           ep = ru_mul(ru_mul(f, ru_mul(ph[a], ph[a])), bT[k]);
         } else {
           const int a = (k + 1) / 2;
-          double f = ru_add(ru_add(ru_add(ca[a], ca[a - 1]), ru_mul(ca[a], ca[a - 1])),
-                            ru_mul(g64, ru_mul(ru_add(1.0, ca[a]), ru_add(1.0, ca[a - 1]))));
+          double f = ru_add(ru_add(ru_add(ru_mul(ca[a], ta[a - 1]), ru_mul(ca[a - 1], ta[a])),
+                                   ru_mul(ca[a], ca[a - 1])),
+                            ru_mul(g64, ru_mul(ru_add(ta[a], ca[a]), ru_add(ta[a - 1], ca[a - 1]))));
           ep = ru_mul(ru_mul(f, ru_mul(ph[a], ph[a - 1])), bT[k]);
         }
         cball g{cscale(ld_c(acc_p + 2 * k), 0.5), ru_mul(0.5, ep)};
         if (loop) {
           const int aa = (k - 1) >> 1, bb = k - 1 - aa;
-          double f = ru_add(ru_add(ru_add(ka[aa], ka[bb]), ru_mul(ka[aa], ka[bb])),
-                            ru_mul(gv, ru_mul(ru_add(1.0, ka[aa]), ru_add(1.0, ka[bb]))));
+          double f = ru_add(ru_add(ru_add(ru_mul(ka[aa], ta[bb]), ru_mul(ka[bb], ta[aa])), ru_mul(ka[aa], ka[bb])),
+                            ru_mul(gv, ru_mul(ru_add(ta[aa], ka[aa]), ru_add(ta[bb], ka[bb]))));
           double evb = ru_mul(0.5, ru_mul(ru_mul(f, ru_mul(ph[aa], ph[bb])), bV[k]));
           g = cb_add(g, cb_scale(cball{ld_c(acc_v + 2 * k), evb}, (double)k));
         }
@@ -649,7 +672,7 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     return cball{mkc(0.0, 0.0), 0.0};
   } else {
     cplx coeff = ld_c(ev + 2 * n);
-    const double rad = eb[0];
+    const double rad = __any_sync(0xffffffffu, tiny_halving) ? INFINITY : eb[0];
     __syncwarp();
     return cball{((n - m) & 1) ? cneg(coeff) : coeff, rad};
   }

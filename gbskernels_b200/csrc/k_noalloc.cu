@@ -130,7 +130,8 @@ int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void*
   cudaStream_t st = (cudaStream_t)stream;
   if (batch < 0 || N < 0) { set_err("gbs_haf_noalloc: negative size"); return (int)cudaErrorInvalidValue; }
   if (batch == 0) return 0;
-  if (!d_mats || !d_out) { set_err("gbs_haf_noalloc: null device pointer"); return (int)cudaErrorInvalidValue; }
+  // an empty matrix (N = 0) has no entries to read: its input pointer may be null
+  if (!d_out || (!d_mats && N > 0)) { set_err("gbs_haf_noalloc: null device pointer"); return (int)cudaErrorInvalidValue; }
   if (N > kHafMaxN) { set_err("gbs_haf_noalloc: N above 32"); return (int)cudaErrorInvalidValue; }
   if (batch > kNoAllocMaxInstances) {
     set_err("gbs_haf_noalloc: batch above 16384");

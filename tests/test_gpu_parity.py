@@ -408,3 +408,34 @@ def test_certified_ladder_in_library(gpu, lib, orc):
     assert all(x["escalated"] and x["tier"] == "certified-dd" for x in d)
     with pytest.raises(FloatingPointError, match="rtol"):
         gpu.haf_batched(mats, precision="certified", return_diagnostics=True, rtol=1e-30)
+
+
+@pytest.mark.parametrize("N", [10, 14])
+def test_nonsymmetric_input_matches_the_reference_formula(gpu, orc, lib, N):
+    """A matrix off symmetry by an antisymmetric E (|E| ~ 1e-9): the reference's
+    power trace of the raw entries (n - 1 products; the binary128 oracle) is even in
+    E, so it moves by O(|E|^2) only.  The kernels evaluate the symmetric part (the
+    half-power identities need B_S symmetric), which must agree with it to the
+    tier's accuracy -- a first-order error in E would show at 1e-9 -- and the
+    certified double-double radius must enclose it."""
+    import ctypes
+    g = np.random.default_rng(31)
+    A = sym(N)
+    X = g.standard_normal((N, N)) + 1j * g.standard_normal((N, N))
+    B = A + 1e-9 * (X - X.T)
+    np.fill_diagonal(B, 0.3 + 0.1j * np.arange(N) / N)
+    for func in ("haf", "lhaf"):
+        t = getattr(orc, func)(B, "quad")
+        fp = getattr(gpu, f"{func}_batched")(B[None])[0]
+        dd = getattr(gpu, f"{func}_batched")(B[None], precision="dd")[0]
+        assert rel_err(fp, t) < 1e-12, (func, rel_err(fp, t))
+        assert rel_err(dd, t) < 4e-16, (func, rel_err(dd, t))
+        out = np.empty(1, np.complex128)
+        bnd = np.empty(1)
+        dp = ctypes.POINTER(ctypes.c_double)
+        Bc = np.ascontiguousarray(B[None])
+        assert getattr(lib, f"gbs_{func}_dd_certified_host")(Bc.ctypes.data_as(dp), N, 1, out.ctypes.data_as(dp),
+                                                             bnd.ctypes.data_as(dp)) == 0
+        assert abs(out[0] - t) <= bnd[0] * (1 + 1e-12), (func, abs(out[0] - t), bnd[0])
+        v, d = getattr(gpu, f"{func}_batched")(B[None], precision="certified", return_diagnostics=True)
+        assert abs(v[0] - t) <= d[0]["abs_error_bound"], (func, d[0])

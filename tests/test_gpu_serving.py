@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 def test_served_equals_alone_bitwise(gpu):
     reqs = workloads.serving_stream(300, rate=1e5, seed=11, nmax=20)
-    with gpu.Server(slots=3, budget_bytes=1 << 20) as srv:
+    with gpu.Server(slots=3, budget_bytes=1 << 17) as srv:
         tickets = [srv.submit(f, m, p) for _, f, p, m in reqs]
         served = [srv.result(t) for t in tickets]
         st = srv.stats()
