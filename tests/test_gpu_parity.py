@@ -436,6 +436,9 @@ def test_nonsymmetric_input_matches_the_reference_formula(gpu, orc, lib, N):
         Bc = np.ascontiguousarray(B[None])
         assert getattr(lib, f"gbs_{func}_dd_certified_host")(Bc.ctypes.data_as(dp), N, 1, out.ctypes.data_as(dp),
                                                              bnd.ctypes.data_as(dp)) == 0
-        assert abs(out[0] - t) <= bnd[0] * (1 + 1e-12), (func, abs(out[0] - t), bnd[0])
+        # t is the binary128 truth rounded to binary64: its own rounding (<= u|t|) is
+        # the slack beside the rigorous radius
+        slack = 2.0 ** -53 * abs(t)
+        assert abs(out[0] - t) <= bnd[0] * (1 + 1e-12) + slack, (func, abs(out[0] - t), bnd[0])
         v, d = getattr(gpu, f"{func}_batched")(B[None], precision="certified", return_diagnostics=True)
-        assert abs(v[0] - t) <= d[0]["abs_error_bound"], (func, d[0])
+        assert abs(v[0] - t) <= d[0]["abs_error_bound"] + slack, (func, d[0])
