@@ -79,6 +79,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_lhaf_repeated_last_error": ([], ctypes.c_char_p),
     "gbs_probe_fp64_peak": ([_dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "gbs_probe_fp64_mma": ([ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+    "gbs_probe_fp64_mma_chains": ([ctypes.c_int] * 4 + [_dp, _dp], ctypes.c_int),
     "gbs_haf_noalloc": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp], ctypes.c_int),
     "gbs_haf_noalloc_last_error": ([], ctypes.c_char_p),
 }

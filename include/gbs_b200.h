@@ -276,6 +276,12 @@ int gbs_probe_fp64_peak(double* tflops, float* ms);
 /* the same probe for one mma shape: k = 8 (m16n8k8, = gbs_probe_fp64_peak) or
  * k = 4 (m16n8k4); flops counted per shape.  No reference counterpart.           */
 int gbs_probe_fp64_mma(int k, double* tflops, float* ms);
+/* the probe as a sweep: k = 8 or 4, chains_per_warp in {1, 2, 4, 8} independent
+ * accumulator chains, warps_per_block (1..16) warps in each of `blocks` blocks;
+ * *cycles = cycles per mma of warp 0 (clock64), its latency when chains = 1.
+ * No reference counterpart.                                                      */
+int gbs_probe_fp64_mma_chains(int k, int chains_per_warp, int warps_per_block, int blocks, double* tflops,
+                              double* cycles);
 
 #ifdef __cplusplus
 }
