@@ -642,6 +642,25 @@ class Workspace:
         _raise_for(rc, f"Workspace.{func}_batched")
         return out
 
+    def evaluate_full(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str]):
+        """As `evaluate`, returning (values, aux, status): aux is sum|term| for the
+        'kappa' tier and the rigorous bound for 'certified' (0 otherwise)."""
+        self._require()
+        B = len(mats)
+        out = np.empty(B, dtype=np.complex128)
+        st = np.zeros(B, dtype=np.int32)
+        aux = np.zeros(B, dtype=np.float64)
+        if B:
+            buf, dims, offs = _pack(mats)
+            fns = np.array([_FN[f] for f in funcs], dtype=np.int32)
+            tiers = np.array([_TIER[p] for p in precisions], dtype=np.int32)
+            rc = _lib.load().gbs_queue_evaluate(
+                self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims), _lib.llptr(offs),
+                _lib.dptr(buf.view(np.float64)), 0 if self._persistent else 1,
+                _lib.dptr(out.view(np.float64)), _lib.dptr(aux), _lib.iptr(st))
+            _lib.check(rc, "gbs_queue_evaluate")
+        return out, aux, st
+
     def evaluate(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str],
                  return_status: bool = False):
         """Mixed-function, mixed-tier, ragged batch in one persistent launch (or per-size
