@@ -541,6 +541,30 @@ def _pack(mats: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     return buf, dims, offsets
 
 
+_C128 = np.dtype(np.complex128)
+
+
+def _pointers(mats) -> tuple[np.ndarray, np.ndarray, list]:
+    """Host pointer and side of every matrix, for the pointer entry points: a
+    C-contiguous complex128 array is passed as it is, anything else is converted
+    first (the converted arrays are returned so they outlive the call).  Raises
+    ValueError naming the first matrix that is not square 2-D."""
+    B = len(mats)
+    ptr = np.empty(B, dtype=np.uint64)
+    dims = np.empty(B, dtype=np.int32)
+    keep = []
+    for i, m in enumerate(mats):
+        if not (type(m) is np.ndarray and m.dtype == _C128 and m.flags.c_contiguous):
+            m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128))
+            keep.append(m)
+        sh = m.shape
+        if len(sh) != 2 or sh[0] != sh[1]:
+            raise ValueError(f"Workspace: matrix #{i} must be square 2-D; got shape {sh}")
+        dims[i] = sh[0]
+        ptr[i] = m.ctypes.data
+    return ptr, dims, keep
+
+
 class Workspace:
     """Device-resident, bucketing session for ragged, sampler-shaped workloads
     (gbskernels/__init__.py:734-908).  One C++ session (stream, monotonically grown
@@ -619,26 +643,29 @@ class Workspace:
             raise NotImplementedError("'ref' is the mpmath ground truth -- CPU only (backend='cpu').")
         if precision not in ("fp64", "dd", "auto"):
             raise ValueError(f"unknown precision {precision!r} for a ragged batch; expected fp64, dd or auto")
-        mats = _as_square_list(matrices)
+        mats = matrices if isinstance(matrices, list) else list(matrices)
         B = len(mats)
         out = np.empty(B, dtype=np.complex128)
         if B == 0:
             return out
-        buf, dims, offs = _pack(mats)
         fns = np.full(B, _FN[func], dtype=np.int32)
         lib = _lib.load()
-        if precision == "auto":
-            kappa = np.empty(B)
-            tier = np.zeros(B, dtype=np.int32)
-            rc = lib.gbs_queue_evaluate_auto(self._session, B, _lib.iptr(fns), _lib.iptr(dims), _lib.llptr(offs),
-                                             _lib.dptr(buf.view(np.float64)), _AUTO_KAPPA_MAX,
-                                             _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier),
-                                             None)
-        else:
+        if precision != "auto":
+            ptr, dims, keep = _pointers(mats)
             tiers = np.full(B, _TIER[precision], dtype=np.int32)
-            rc = lib.gbs_queue_evaluate(self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims),
-                                        _lib.llptr(offs), _lib.dptr(buf.view(np.float64)),
-                                        0 if self._persistent else 1, _lib.dptr(out.view(np.float64)), None, None)
+            rc = lib.gbs_queue_evaluate_ptrs(self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims),
+                                             ctypes.c_void_p(ptr.ctypes.data), 0 if self._persistent else 1,
+                                             _lib.dptr(out.view(np.float64)), None, None)
+            del keep
+            _raise_for(rc, f"Workspace.{func}_batched")
+            return out
+        mats = _as_square_list(mats)
+        buf, dims, offs = _pack(mats)
+        kappa = np.empty(B)
+        tier = np.zeros(B, dtype=np.int32)
+        rc = lib.gbs_queue_evaluate_auto(self._session, B, _lib.iptr(fns), _lib.iptr(dims), _lib.llptr(offs),
+                                         _lib.dptr(buf.view(np.float64)), _AUTO_KAPPA_MAX,
+                                         _lib.dptr(out.view(np.float64)), _lib.dptr(kappa), _lib.iptr(tier), None)
         _raise_for(rc, f"Workspace.{func}_batched")
         return out
 
@@ -651,15 +678,19 @@ class Workspace:
         st = np.zeros(B, dtype=np.int32)
         aux = np.zeros(B, dtype=np.float64)
         if B:
-            buf, dims, offs = _pack(mats)
-            fns = np.array([_FN[f] for f in funcs], dtype=np.int32)
-            tiers = np.array([_TIER[p] for p in precisions], dtype=np.int32)
-            rc = _lib.load().gbs_queue_evaluate(
-                self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims), _lib.llptr(offs),
-                _lib.dptr(buf.view(np.float64)), 0 if self._persistent else 1,
-                _lib.dptr(out.view(np.float64)), _lib.dptr(aux), _lib.iptr(st))
-            _lib.check(rc, "gbs_queue_evaluate")
+            self._call_ptrs(funcs, mats, precisions, out, aux, st)
         return out, aux, st
+
+    def _call_ptrs(self, funcs, mats, precisions, out, aux, st) -> None:
+        ptr, dims, keep = _pointers(mats)
+        fns = np.array([_FN[f] for f in funcs], dtype=np.int32)
+        tiers = np.array([_TIER[p] for p in precisions], dtype=np.int32)
+        rc = _lib.load().gbs_queue_evaluate_ptrs(
+            self._session, len(mats), _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims),
+            ctypes.c_void_p(ptr.ctypes.data), 0 if self._persistent else 1,
+            _lib.dptr(out.view(np.float64)), _lib.dptr(aux), _lib.iptr(st))
+        del keep
+        _lib.check(rc, "gbs_queue_evaluate_ptrs")
 
     def evaluate(self, funcs: list[str], mats: list[np.ndarray], precisions: list[str],
                  return_status: bool = False):
@@ -672,14 +703,7 @@ class Workspace:
         aux = np.zeros(B, dtype=np.float64)
         if B == 0:
             return (out, st) if return_status else out
-        buf, dims, offs = _pack(mats)
-        fns = np.array([_FN[f] for f in funcs], dtype=np.int32)
-        tiers = np.array([_TIER[p] for p in precisions], dtype=np.int32)
-        rc = _lib.load().gbs_queue_evaluate(
-            self._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims), _lib.llptr(offs),
-            _lib.dptr(buf.view(np.float64)), 0 if self._persistent else 1,
-            _lib.dptr(out.view(np.float64)), _lib.dptr(aux), _lib.iptr(st))
-        _lib.check(rc, "gbs_queue_evaluate")
+        self._call_ptrs(funcs, mats, precisions, out, aux, st)
         return (out, st) if return_status else out
 
     # device-resident outputs (uniform batches)

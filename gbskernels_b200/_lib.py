@@ -62,6 +62,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_dev_free": ([_dp], ctypes.c_int),
     "gbs_queue_evaluate": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int, _dp, _dp, _ip],
                            ctypes.c_int),
+    "gbs_queue_evaluate_ptrs": ([_vp, ctypes.c_int, _ip, _ip, _ip, _vp, ctypes.c_int, _dp, _dp, _ip],
+                                ctypes.c_int),
     "gbs_session_last_stats": ([_vp, _dp, _ip, _llp], ctypes.c_int),
     "gbs_queue_prepare": ([_vp, ctypes.c_int, _ip, _ip, _ip, _llp, _dp, ctypes.c_int], ctypes.c_int),
     "gbs_queue_run": ([_vp, _vp], ctypes.c_int),

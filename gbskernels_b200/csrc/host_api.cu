@@ -23,6 +23,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gbs_kernels.cuh"
@@ -553,25 +554,56 @@ static int plan_build(gbs_session* s, const std::vector<Req>& reqs, const RunOpt
     double* dst = (double*)s->pin_in.p;
     s->gdesc.clear();
     s->gidx.clear();
+    std::vector<int> host_rows;  // requests copied from host memory
+    host_rows.reserve(B);
     for (int i = 0; i < B; ++i) {
       if (s->plan_trivial[i]) continue;
-      const long long o = off[i];
       const int d = reqs[i].dim, de = dim_eval[i];
       if (reqs[i].state) {  // filled on the device by the gather kernel
-        GatherDesc gd{o, (long long)s->gidx.size(), reqs[i].state, reqs[i].gamma, d, de, reqs[i].M,
+        GatherDesc gd{off[i], (long long)s->gidx.size(), reqs[i].state, reqs[i].gamma, d, de, reqs[i].M,
                       reqs[i].gamma != nullptr};
         s->gdesc.push_back(gd);
         s->gidx.insert(s->gidx.end(), reqs[i].idx, reqs[i].idx + d);
         continue;
       }
-      if (de == d) {
-        std::memcpy(dst + o, reqs[i].mat, sizeof(double) * 2 * (size_t)d * d);
-      } else {
-        std::memset(dst + o, 0, sizeof(double) * 2 * (size_t)de * de);
-        for (int r = 0; r < d; ++r)
-          std::memcpy(dst + o + 2ll * r * de, reqs[i].mat + 2ll * r * d, sizeof(double) * 2 * d);
-        dst[o + 2ll * ((long long)d * de + d)] = 1.0;
+      host_rows.push_back(i);
+    }
+    auto pack = [&](size_t lo, size_t hi) {
+      for (size_t k = lo; k < hi; ++k) {
+        const int i = host_rows[k];
+        const long long o = off[i];
+        const int d = reqs[i].dim, de = dim_eval[i];
+        if (de == d) {
+          std::memcpy(dst + o, reqs[i].mat, sizeof(double) * 2 * (size_t)d * d);
+        } else {
+          std::memset(dst + o, 0, sizeof(double) * 2 * (size_t)de * de);
+          for (int r = 0; r < d; ++r)
+            std::memcpy(dst + o + 2ll * r * de, reqs[i].mat + 2ll * r * d, sizeof(double) * 2 * d);
+          dst[o + 2ll * ((long long)d * de + d)] = 1.0;
+        }
       }
+    };
+    // a large batch is packed by several host threads (disjoint ranges of requests,
+    // disjoint destination ranges): one thread copies a few GB/s, short of what the
+    // upload that follows moves
+    const size_t bytes = (size_t)std::max<long long>(mat_doubles, 0) * sizeof(double);
+    const int nth = (int)std::min<size_t>({(size_t)std::max(1u, std::thread::hardware_concurrency()), (size_t)8,
+                                            bytes / (8u << 20) + 1, host_rows.size() + 1});
+    if (nth <= 1) {
+      pack(0, host_rows.size());
+    } else {
+      std::vector<std::thread> th;
+      const size_t per = (host_rows.size() + nth - 1) / nth;
+      for (int t = 0; t < nth; ++t) {
+        const size_t lo = std::min(host_rows.size(), t * per), hi = std::min(host_rows.size(), lo + per);
+        if (lo >= hi) continue;
+        try {
+          th.emplace_back(pack, lo, hi);
+        } catch (...) {  // no thread to be had: this range in the calling thread
+          pack(lo, hi);
+        }
+      }
+      for (auto& t : th) t.join();
     }
     if (mat_doubles > 0) {
       e = cudaMemcpyAsync(s->mats.p, s->pin_in.p, mat_doubles * sizeof(double), cudaMemcpyHostToDevice, s->stream);
@@ -1328,6 +1360,30 @@ int gbs_queue_evaluate(gbs_session* s, int B, const int* funcs, const int* tiers
   if (!funcs || !tiers || !dims || !offsets || !mats || !out) return fail(cudaErrorInvalidValue, "null buffer");
   std::vector<Req> reqs(B);
   for (int i = 0; i < B; ++i) reqs[i] = Req{funcs[i], tiers[i], dims[i], mats + 2 * offsets[i]};
+  std::vector<int> st(B);
+  RunOpts opt;
+  opt.per_size = (mode == 1);
+  std::lock_guard<std::mutex> lk(s->mu);
+  int rc = run_batch(s, reqs, out, aux, st.data(), opt);
+  if (rc) return rc;
+  if (status) std::memcpy(status, st.data(), sizeof(int) * B);
+  apply_status(B, out, st.data());
+  return 0;
+}
+
+// As gbs_queue_evaluate, with one host pointer per matrix instead of one packed
+// buffer: the matrices are copied once, straight into the session's pinned staging
+// buffer, so a caller holding B separate arrays does not pack them first.
+int gbs_queue_evaluate_ptrs(gbs_session* s, int B, const int* funcs, const int* tiers, const int* dims,
+                            const double* const* mats, int mode, double* out, double* aux, int* status) {
+  if (!s) return fail(cudaErrorInvalidValue, "null session");
+  if (B <= 0) return 0;
+  if (!funcs || !tiers || !dims || !mats || !out) return fail(cudaErrorInvalidValue, "null buffer");
+  std::vector<Req> reqs(B);
+  for (int i = 0; i < B; ++i) {
+    if (!mats[i] && dims[i] > 0) return fail(cudaErrorInvalidValue, "null matrix pointer");
+    reqs[i] = Req{funcs[i], tiers[i], dims[i], mats[i]};
+  }
   std::vector<int> st(B);
   RunOpts opt;
   opt.per_size = (mode == 1);

@@ -199,6 +199,12 @@ int gbs_dev_device(const void* d, int* device);
 int gbs_queue_evaluate(gbs_session* s, int batch, const int* funcs, const int* tiers, const int* dims,
                        const long long* offsets, const double* mats, int mode, double* out, double* aux,
                        int* status);
+/* as gbs_queue_evaluate, with one host pointer per matrix (mats[i]: dims[i]^2
+ * complex, row-major) instead of a packed buffer: each matrix is copied once,
+ * straight into the session's pinned staging buffer.  No reference counterpart
+ * (the reference stacks each size bucket with np.stack, gbskernels/__init__.py:822-833). */
+int gbs_queue_evaluate_ptrs(gbs_session* s, int batch, const int* funcs, const int* tiers, const int* dims,
+                            const double* const* mats, int mode, double* out, double* aux, int* status);
 /* auto tier over a ragged / mixed batch (tiers are implied): fp64 + indicator for
  * every request in one launch, kappa >= kappa_max reruns in double-double in one
  * more; tier_out[i] 0 fp64, 1 dd; kappa[i] = sum|term| / |value|.

@@ -378,6 +378,46 @@ def test_ragged_auto_equals_each_element_alone(gpu):
         assert d["tier"] == ("dd" if m.shape[0] == 8 else "fp64")
 
 
+def test_pointer_entry_equals_packed_buffer(gpu, lib):
+    """gbs_queue_evaluate_ptrs (one host pointer per matrix, the path of
+    Workspace.evaluate) gives bit for bit what gbs_queue_evaluate gives from one
+    packed buffer: ragged sizes, odd loop hafnians (augmented while packing), a
+    permanent and a torontonian, inputs that need converting (a transposed view,
+    real float64), every tier; a matrix that is not square is refused by name."""
+    import ctypes
+    from gbskernels_b200 import _lib
+    g = np.random.default_rng(21)
+    A16 = sym(16)
+    mats = [sym(12), sym(7), A16.T, sym(10).real.copy(), g.standard_normal((9, 9)) + 0j, phys_O(5).astype(complex),
+            sym(20), sym(9), sym(14)]
+    funcs = ["haf", "lhaf", "haf", "lhaf", "perm", "tor", "lhaf", "lhaf", "haf"]
+    for tier_name in ("fp64", "dd", "kappa", "certified"):
+        precs = [tier_name] * len(mats)
+        with gpu.Workspace() as ws:
+            v1, a1, s1 = ws.evaluate_full(funcs, mats, precs)
+            conv = [np.ascontiguousarray(np.asarray(m, dtype=np.complex128)) for m in mats]
+            buf, dims, offs = gpu._pack(conv)
+            B = len(mats)
+            v2 = np.empty(B, np.complex128)
+            a2 = np.zeros(B)
+            s2 = np.zeros(B, np.int32)
+            fns = np.array([gpu._FN[f] for f in funcs], np.int32)
+            tiers = np.array([gpu._TIER[p] for p in precs], np.int32)
+            _lib.check(lib.gbs_queue_evaluate(ws._session, B, _lib.iptr(fns), _lib.iptr(tiers), _lib.iptr(dims),
+                                              _lib.llptr(offs), _lib.dptr(buf.view(np.float64)), 0,
+                                              _lib.dptr(v2.view(np.float64)), _lib.dptr(a2), _lib.iptr(s2)), "packed")
+        assert np.array_equal(v1, v2, equal_nan=True), tier_name
+        assert np.array_equal(a1, a2, equal_nan=True), tier_name
+        assert np.array_equal(s1, s2), tier_name
+    with gpu.Workspace() as ws:
+        with pytest.raises(ValueError, match="matrix #1 must be square"):
+            ws.evaluate(["haf", "haf"], [sym(6), np.zeros((4, 6), complex)], ["fp64", "fp64"])
+        rag_in = [sym(8), sym(12).T, sym(6)]
+        ragged = ws.haf_batched(rag_in, precision="dd")
+    for i, m in enumerate(rag_in):
+        assert ragged[i] == gpu.haf(np.ascontiguousarray(m), precision="dd"), i
+
+
 def test_certified_ladder_in_library(gpu, lib, orc):
     """gbs_certified_ladder_host: an rtol the binary64 certificate meets keeps it
     (tier 3); a tighter one escalates to the certified double-double rung (tier 4,
