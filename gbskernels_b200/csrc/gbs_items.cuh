@@ -95,7 +95,10 @@ __device__ ItemResult perm_item(const double* __restrict__ mats, const InstDesc&
   return r;
 }
 
-template <int TIER>
+// REAL: the instance is real (binary64 tiers; the host sets InstDesc::real_in) and
+// runs the real power loop.  A separate instantiation, so the complex code is
+// compiled as if the real path did not exist.
+template <int TIER, bool REAL = false>
 __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, const InstDesc& d, const WorkItem& w,
                                bool loop, double* ws, int haf_smax, int lane) {
   ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStOk};
@@ -128,7 +131,7 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     cball acc{mkc(0.0, 0.0), 0.0};
     int cnt = 0;
     for (unsigned long long k = 0; k < w.count; ++k) {
-      cball t = haf_subset_term_tc<true>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
+      cball t = haf_subset_term_tc<true, REAL>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
       if (lane == 0) {
         ring[cnt * 3] = t.z.re;
         ring[cnt * 3 + 1] = t.z.im;
@@ -155,7 +158,7 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     double absacc = 0.0;
     int cnt = 0;
     for (unsigned long long k = 0; k < w.count; ++k) {
-      haf_subset_term_tc<false>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane, ring + cnt * L.slot * 2);
+      haf_subset_term_tc<false, REAL>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane, ring + cnt * L.slot * 2);
       if (++cnt == kHafRing || k + 1 == w.count) {
         __syncwarp();
         double ab = 0.0;
@@ -287,6 +290,10 @@ __device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstD
                                                 double* ws, int lane) {
   ItemResult r{ddc{dd_make(0.0), dd_make(0.0)}, 0.0, kStTooLarge};
   switch (d.ft) {
+// binary64 hafnian tiers: the real instantiation for a real instance
+#define GBSB_HAF(TIER, LOOP)                                                     \
+  (d.real_in ? haf_item<TIER, true>(P.mats, d, w, LOOP, ws, P.haf_smax, lane)   \
+             : haf_item<TIER, false>(P.mats, d, w, LOOP, ws, P.haf_smax, lane))
 #define GBSB_BR(FN, TIER, CALL) \
   case ft_code(FN, TIER):         \
     if constexpr ((BR >> ft_code(FN, TIER)) & 1u) { r = CALL; } \
@@ -294,24 +301,25 @@ __device__ __forceinline__ ItemResult eval_item(const ItemLaunch& P, const InstD
     GBSB_BR(kFnPerm, kTierFp64, (perm_item<kTierFp64>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnPerm, kTierKappa, (perm_item<kTierKappa>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnPerm, kTierDD, (perm_item<kTierDD>(P.mats, d, w, ws, lane)))
-    GBSB_BR(kFnHaf, kTierFp64, (haf_item<kTierFp64>(P.mats, d, w, false, ws, P.haf_smax, lane)))
-    GBSB_BR(kFnHaf, kTierKappa, (haf_item<kTierKappa>(P.mats, d, w, false, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnHaf, kTierFp64, (GBSB_HAF(kTierFp64, false)))
+    GBSB_BR(kFnHaf, kTierKappa, (GBSB_HAF(kTierKappa, false)))
     GBSB_BR(kFnHaf, kTierDD, (haf_item<kTierDD>(P.mats, d, w, false, ws, P.haf_smax, lane)))
-    GBSB_BR(kFnLhaf, kTierFp64, (haf_item<kTierFp64>(P.mats, d, w, true, ws, P.haf_smax, lane)))
-    GBSB_BR(kFnLhaf, kTierKappa, (haf_item<kTierKappa>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnLhaf, kTierFp64, (GBSB_HAF(kTierFp64, true)))
+    GBSB_BR(kFnLhaf, kTierKappa, (GBSB_HAF(kTierKappa, true)))
     GBSB_BR(kFnLhaf, kTierDD, (haf_item<kTierDD>(P.mats, d, w, true, ws, P.haf_smax, lane)))
     GBSB_BR(kFnTor, kTierFp64, (tor_item<kTierFp64>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierKappa, (tor_item<kTierKappa>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierDD, (tor_item<kTierDD>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnPerm, kTierCert, (perm_item<kTierCert>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnPerm, kTierCertDD, (perm_item<kTierCertDD>(P.mats, d, w, ws, lane)))
-    GBSB_BR(kFnHaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, false, ws, P.haf_smax, lane)))
-    GBSB_BR(kFnLhaf, kTierCert, (haf_item<kTierCert>(P.mats, d, w, true, ws, P.haf_smax, lane)))
+    GBSB_BR(kFnHaf, kTierCert, (GBSB_HAF(kTierCert, false)))
+    GBSB_BR(kFnLhaf, kTierCert, (GBSB_HAF(kTierCert, true)))
     GBSB_BR(kFnHaf, kTierCertDD, (haf_item<kTierCertDD>(P.mats, d, w, false, ws, P.haf_smax, lane)))
     GBSB_BR(kFnLhaf, kTierCertDD, (haf_item<kTierCertDD>(P.mats, d, w, true, ws, P.haf_smax, lane)))
     GBSB_BR(kFnTor, kTierCert, (tor_item<kTierCert>(P.mats, d, w, ws, lane)))
     GBSB_BR(kFnTor, kTierCertDD, (tor_item<kTierCertDD>(P.mats, d, w, ws, lane)))
 #undef GBSB_BR
+#undef GBSB_HAF
     default:
       break;
   }

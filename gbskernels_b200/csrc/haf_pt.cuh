@@ -467,13 +467,297 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
 }
 
 // ---------------------------------------------------------------------------
+// Real inputs (every imaginary part zero).  B_S and C = B_S X are real, so the
+// powers need none of the complex embedding: real m16n8k8 products with K = s (not
+// 2s) over s columns (not 2s), a quarter of the mma work, and real traces.  The
+// identities, the half-power schedule and the trace accumulators (acc_p, acc_v:
+// real parts, imaginary parts zero) are those of the complex path.
+//
+// Real mma fragment layout (m16n8k8 .f64): A rows g / g+8, columns t4 / t4+4;
+// B rows t4 / t4+4, column g; accumulator rows g / g+8, columns 2 t4 / 2 t4 + 1.
+// The trace partner (i^1, t^1) of a lane's element (g, 2t4) is (g^1, 2t4+1): lane ^ 4,
+// the other register of the pair.
+
+// Row stride (doubles) of the real C and power: at least the K padding (a multiple
+// of 8) and == 4 (mod 16), which spreads both fragment loads over the 16 8-byte
+// bank pairs of a half warp (rows t4 or g step by 4 banks pairs).
+__host__ __device__ inline int haf_r_stride(int s) {
+  const int k = (s + 7) & ~7;
+  return ((k + 11) / 16) * 16 + 4;
+}
+struct HafRealLayout {
+  int rs;                                    // row stride (doubles)
+  int c_off, p_off, y_off, d_off, total;     // in doubles, from the real scratch base
+};
+__host__ __device__ inline HafRealLayout haf_real_layout(int smax) {
+  HafRealLayout L;
+  if (smax < 2) smax = 2;
+  L.rs = haf_r_stride(smax);
+  const int rows = 16 * haf_strips(smax);
+  const int h = (smax / 2 + 1) / 2;
+  L.c_off = 0;
+  L.p_off = rows * L.rs;                     // C (rows and columns zero-padded)
+  L.y_off = L.p_off + 16 * L.rs;             // the power of one strip
+  L.d_off = L.y_off + 16 * (h + 1);          // the loop vectors of one strip
+  L.total = L.d_off + L.rs;                  // d (zero beyond s)
+  L.total = (L.total + 1) & ~1;
+  return L;
+}
+
+// D = P * C on the real tiles in use (ntr of up to NT tiles of 8 columns), K = s:
+// s / 8 m16n8k8 steps, then an m16n8k4 step when s % 8 <= 4, or one more m16n8k8
+// step over zero-padded columns when s % 8 == 6.
+template <int NT>
+__device__ __forceinline__ void power_product_real(const double* __restrict__ P, const double* __restrict__ Cr, int s,
+                                                   int rs, int ntr, int lane, double (&D)[NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) D[nt][0] = D[nt][1] = D[nt][2] = D[nt][3] = 0.0;
+  const double* ap = P + g * rs + t4;
+  const double* bp = Cr + t4 * rs + g;
+  const int n8 = (s + 2) >> 3;  // s % 8 == 6 rounds up to one more k8 step
+#pragma unroll 1
+  for (int j = 0; j < n8; ++j) {
+    const int k0 = 8 * j;
+    const double a0 = ap[k0], a1 = ap[8 * rs + k0], a2 = ap[k0 + 4], a3 = ap[8 * rs + k0 + 4];
+    const double* b0p = bp + k0 * rs;
+    const double* b1p = bp + (k0 + 4) * rs;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+      if (nt < ntr) dmma_m16n8k8(D[nt], a0, a1, a2, a3, b0p[8 * nt], b1p[8 * nt]);
+  }
+  if ((s & 7) != 0 && (s & 7) <= 4) {
+    const int k0 = 8 * n8;
+    const double a0 = ap[k0], a1 = ap[8 * rs + k0];
+    const double* b0p = bp + k0 * rs;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+      if (nt < ntr) dmma_m16n8k4(D[nt], a0, a1, b0p[8 * nt]);
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void load_acc_real(const double* P, int rs, int ntr, int lane, double (&D)[NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    cplx x0 = mkc(0.0, 0.0), x1 = mkc(0.0, 0.0);
+    if (nt < ntr) {
+      x0 = ld_c(P + g * rs + 8 * nt + 2 * t4);
+      x1 = ld_c(P + (g + 8) * rs + 8 * nt + 2 * t4);
+    }
+    D[nt][0] = x0.re; D[nt][1] = x0.im; D[nt][2] = x1.re; D[nt][3] = x1.im;
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void store_acc_real(double* P, int rs, int ntr, int lane, const double (&D)[NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt)
+    if (nt < ntr) {
+      st_c(P + g * rs + 8 * nt + 2 * t4, mkc(D[nt][0], D[nt][1]));
+      st_c(P + (g + 8) * rs + 8 * nt + 2 * t4, mkc(D[nt][2], D[nt][3]));
+    }
+}
+
+// Lane partial of sum_{i,t} D[i][t] D[i^1][t^1] (partner: lane ^ 4, other register).
+template <int NT>
+__device__ __forceinline__ double even_partial_real(const double (&D)[NT][4], int ntr) {
+  double e0 = 0.0, e1 = 0.0;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    if (nt >= ntr) continue;
+    const double p0 = shfl_xor_d(D[nt][0], 4), p1 = shfl_xor_d(D[nt][1], 4);
+    const double p2 = shfl_xor_d(D[nt][2], 4), p3 = shfl_xor_d(D[nt][3], 4);
+    e0 = fma(D[nt][0], p1, e0);
+    e1 = fma(D[nt][1], p0, e1);
+    e0 = fma(D[nt][2], p3, e0);
+    e1 = fma(D[nt][3], p2, e1);
+  }
+  return e0 + e1;
+}
+
+// Lane partial of sum_{i,t} D[i][t] Q[i^1][t^1], Q the previous power (stride rs).
+template <int NT>
+__device__ __forceinline__ double odd_partial_real(const double (&D)[NT][4], const double* Q, int rs, int ntr,
+                                                   int lane) {
+  const int g = lane >> 2, t4 = lane & 3;
+  double o0 = 0.0, o1 = 0.0;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    if (nt >= ntr) continue;
+    const cplx q0 = ld_c(Q + (g ^ 1) * rs + 8 * nt + 2 * t4);
+    const cplx q1 = ld_c(Q + ((g + 8) ^ 1) * rs + 8 * nt + 2 * t4);
+    o0 = fma(D[nt][0], q0.im, o0);
+    o1 = fma(D[nt][1], q0.re, o1);
+    o0 = fma(D[nt][2], q1.im, o0);
+    o1 = fma(D[nt][3], q1.re, o1);
+  }
+  return o0 + o1;
+}
+
+// y[row] = sum_t D[row][t] d[t] for the rows of this lane's group; lanes t4 == 0
+// write Y[row * hp1 + col].
+template <int NT>
+__device__ __forceinline__ void rows_times_d_real(const double (&D)[NT][4], const double* Dr, double* Y, int col,
+                                                  int hp1, int ntr, int lane) {
+  const int g = lane >> 2, t4 = lane & 3;
+  double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    if (nt >= ntr) continue;
+    const cplx dv = ld_c(Dr + 8 * nt + 2 * t4);
+    y0 = fma(D[nt][0], dv.re, y0);
+    y0 = fma(D[nt][1], dv.im, y0);
+    y1 = fma(D[nt][2], dv.re, y1);
+    y1 = fma(D[nt][3], dv.im, y1);
+  }
+#pragma unroll
+  for (int m = 1; m <= 2; m <<= 1) {
+    y0 += shfl_xor_d(y0, m);
+    y1 += shfl_xor_d(y1, m);
+  }
+  if (t4 == 0) {
+    Y[g * hp1 + col] = y0;
+    Y[(g + 8) * hp1 + col] = y1;
+  }
+}
+
+// Sum of two values over the warp: lanes with (lane >> 4) & 1 == b get the total of
+// value b (5 shuffles).
+__device__ __forceinline__ double warp_sum2_scatter(double v0, double v1, int lane) {
+  const bool b4 = (lane & 16) != 0;
+  double k = b4 ? v1 : v0;
+  k += shfl_xor_d(b4 ? v0 : v1, 16);
+  k += shfl_xor_d(k, 8);
+  k += shfl_xor_d(k, 4);
+  k += shfl_xor_d(k, 2);
+  k += shfl_xor_d(k, 1);
+  return k;
+}
+
+// The power loop of one real subset: the 16-row strips run their chains in turn
+// (as haf_powers); traces go to the real parts of acc_p[k], the loop terms to acc_v[k].
+template <int NT>
+__device__ __noinline__ void haf_powers_real(const double* Cr, double* P, double* Y, const double* Dr, double* acc_p,
+                                             double* acc_v, int s, int rs, int n, int h, bool loop, int lane) {
+  const int ntr = (s + 7) >> 3;  // real column tiles in use (<= NT)
+  const int hp1 = h + 1;
+  const int strips = haf_strips(s);
+  const bool lead = (lane & 15) == 0;  // lane 0: the odd total, lane 16: the even total
+  const int half = lane >> 4;
+  for (int ms = 0; ms < strips; ++ms) {
+    const int r0 = 16 * ms;
+    const double* Cstrip = Cr + r0 * rs;
+    double D[NT][4];
+    if (loop && lane < 16) Y[lane * hp1] = r0 + lane < s ? Dr[r0 + lane] : 0.0;
+    load_acc_real<NT>(Cstrip, rs, ntr, lane, D);
+    {
+      const double tot = warp_sum_d(even_partial_real<NT>(D, ntr));
+      if (lane == 0 && 2 <= n) acc_p[4] += tot;
+    }
+    if (loop) rows_times_d_real<NT>(D, Dr, Y, 1, hp1, ntr, lane);
+    for (int a = 2; a <= h; ++a) {
+      const double* Q = (a == 2) ? Cstrip : P;
+      power_product_real<NT>(Q, Cr, s, rs, ntr, lane, D);
+      const double to = odd_partial_real<NT>(D, Q, rs, ntr, lane);
+      const double te = even_partial_real<NT>(D, ntr);
+      const double tot = warp_sum2_scatter(to, te, lane);
+      if (lead) {
+        const int k = half == 0 ? 2 * a - 1 : 2 * a;
+        if (k <= n) acc_p[2 * k] += tot;
+      }
+      __syncwarp();
+      store_acc_real<NT>(P, rs, ntr, lane, D);
+      if (loop) rows_times_d_real<NT>(D, Dr, Y, a, hp1, ntr, lane);
+      __syncwarp();
+    }
+    if (loop) {
+      __syncwarp();
+      if (lane < n) {
+        const int k = lane + 1;
+        const int aa = (k - 1) >> 1, bb = k - 1 - aa;
+        const int nr = min(16, s - r0);
+        double t = 0.0;
+        for (int i = 0; i < nr; ++i) t = fma(Y[(i ^ 1) * hp1 + aa], Y[i * hp1 + bb], t);
+        acc_v[2 * k] += 0.5 * t;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Stage the real C = B_S X (symmetric part, rows and columns zero-padded to the
+// tiles read) and d for a real subset into the real scratch (after the layout's
+// own areas); the certified tier also gets |C| and d in the complex layout, which
+// its bound path reads.  Returns this lane's "tiny halving" flag (see the complex
+// staging in haf_subset_term_tc).
+// Entry (r, c) of the real C = B_S X as the symmetric part (x + y) / 2; zero outside
+// the s x s block and on the skipped diagonal of a plain hafnian.  `tiny` (certified
+// tier) records a halving that could round absolutely.
+template <bool CERT>
+__device__ __forceinline__ double haf_real_entry(const double* __restrict__ A, int N, int s, bool loop,
+                                                 const int* gi, int r, int c, bool& tiny) {
+  if (r >= s || c >= s) return 0.0;
+  const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
+  if (!loop && rr == cc) return 0.0;
+  const double x = A[((size_t)rr * N + cc) * 2], y = A[((size_t)cc * N + rr) * 2];
+  if constexpr (CERT) {
+    const double w = x + y;
+    if (x != y && fabs(w) > 0.0 && fabs(w) < 4.450147717014403e-308) tiny = true;
+  }
+  return 0.5 * (x + y);
+}
+
+template <bool CERT>
+__device__ __noinline__ bool haf_stage_real(const double* __restrict__ A, int N, int s, bool loop, const int* gi,
+                                            int smax, double* ws, double* rb, int lane) {
+  const HafRealLayout R = haf_real_layout(smax);
+  double* Cr = rb + R.c_off;
+  double* Dr = rb + R.d_off;
+  const int rs = R.rs;
+  const int rows = 16 * haf_strips(s);
+  const int rcols = 8 * ((s + 7) >> 3);
+  bool tiny = false;
+  const int dr = 32 / rcols, dc = 32 - dr * rcols;  // (r, c) advance per 32 elements
+  int r = lane / rcols, c = lane - (lane / rcols) * rcols;
+  for (int e = lane; e < rows * rcols; e += 32, r += dr, c += dc) {
+    if (c >= rcols) {
+      c -= rcols;
+      ++r;
+    }
+    Cr[r * rs + c] = haf_real_entry<CERT>(A, N, s, loop, gi, r, c, tiny);
+  }
+  if (loop)
+    for (int k = lane; k < rs; k += 32) Dr[k] = k < s ? A[((size_t)gi[k] * N + gi[k]) * 2] : 0.0;
+  if constexpr (CERT) {
+    const int cs = haf_c_stride(s);
+    const int ccols = (((2 * s + 7) >> 3) << 2);
+    double* Ca = ws + haf_layout(smax, true).ca_off;
+    const int dr2 = 32 / ccols, dc2 = 32 - dr2 * ccols;
+    int r2 = lane / ccols, c2 = lane - (lane / ccols) * ccols;
+    for (int e = lane; e < rows * ccols; e += 32, r2 += dr2, c2 += dc2) {
+      if (c2 >= ccols) {
+        c2 -= ccols;
+        ++r2;
+      }
+      st_c(Ca + (r2 * cs + c2) * 2, mkc(fabs(haf_real_entry<CERT>(A, N, s, loop, gi, r2, c2, tiny)), 0.0));
+    }
+    if (loop && lane < s)
+      st_c(ws + haf_layout(smax, true).d_off + lane * 2, mkc(A[((size_t)gi[lane] * N + gi[lane]) * 2], 0.0));
+  }
+  return tiny;
+}
+
+// ---------------------------------------------------------------------------
 // Evaluate the signed power-trace term of one subset `mask` of instance A (N x N
 // complex, row-major, N = 2n even).  Returns the same ball in every lane (radius 0
 // unless CERT).  `loop` selects the loop hafnian; `ws` is this warp's workspace.
 // Binary64 tiers (CERT false): kg[1..n] and the sign are parked in the ring slot
 // `slot` (required) instead of running the Newton recurrence (haf_ring_flush runs
 // it for a whole ring); the certified tier runs it in ball arithmetic here.
-template <bool CERT>
+template <bool CERT, bool REAL = false>
 static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, int n, uint32_t mask,
                                            bool loop, double* ws, const HafLayout& Lw, int lane,
                                            double* slot = nullptr) {
@@ -507,8 +791,11 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     gi[lane] = 2 * (__ffs(mm) - 1) + (lane & 1);
   }
   __syncwarp();
+  bool tiny_halving = false;  // certified tier: see the staging below
+  if constexpr (REAL) {
+    tiny_halving = haf_stage_real<CERT>(A, N, s, loop, gi, Lw.smax, ws, ws + Lw.total, lane);
+  } else {
   const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
-  bool tiny_halving = false;                    // certified tier: see the staging below
   // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
   const int dr = 32 / ccols, dc = 32 - dr * ccols;  // (r, c) advance per 32 elements
   int r = lane / ccols, c = lane - (lane / ccols) * ccols;
@@ -541,6 +828,7 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
   }
   if (loop && lane < s) st_c(Dv + lane * 2, ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2));
+  }
   for (int k = lane; k <= n; k += 32) {
     st_c(acc_p + 2 * k, mkc(0.0, 0.0));
     st_c(acc_v + 2 * k, mkc(0.0, 0.0));
@@ -551,7 +839,17 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     if (loop && lane < rows) Ym[lane * hp1] = lane < s ? ru_abs_c(ld_c(Dv + lane * 2)) : 0.0;
   }
   // p_1 = tr(C)
-  {
+  if constexpr (REAL) {
+    const HafRealLayout R = haf_real_layout(Lw.smax);
+    const double* Cr = ws + Lw.total + R.c_off;
+    const double d = lane < s ? Cr[lane * R.rs + lane] : 0.0;
+    const double t = warp_sum_d(d);
+    if (lane == 0) st_c(acc_p + 2, mkc(t, 0.0));
+    if constexpr (CERT) {
+      const double a1 = warp_sum_ru(fabs(d));
+      if (lane == 0) bT[1] = a1;
+    }
+  } else {
     cplx t = mkc(0.0, 0.0);
     if (lane < s) t = ld_c(Cs + (lane * cs + lane) * 2);
     t = warp_sum_c(t);
@@ -571,8 +869,21 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   // mixing the two widths in one launch measured slower (instruction-fetch stalls
   // 2.2 against 0.3 cycles per issue).  Both widths run the same operations on the
   // tiles in use, so a value does not depend on the launch it is part of.
-  if (Lw.smax <= 16) haf_powers<4>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
-  else haf_powers<8>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
+  // A real subset runs its own loop (real tiles of 8 columns: up to 2 for N <= 16,
+  // 4 above) on the real scratch.
+  if constexpr (REAL) {
+    const HafRealLayout R = haf_real_layout(Lw.smax);
+    double* rb = ws + Lw.total;
+    if (Lw.smax <= 16)
+      haf_powers_real<2>(rb + R.c_off, rb + R.p_off, rb + R.y_off, rb + R.d_off, acc_p, acc_v, s, R.rs, n, h, loop,
+                         lane);
+    else
+      haf_powers_real<4>(rb + R.c_off, rb + R.p_off, rb + R.y_off, rb + R.d_off, acc_p, acc_v, s, R.rs, n, h, loop,
+                         lane);
+  } else {
+    if (Lw.smax <= 16) haf_powers<4>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
+    else haf_powers<8>(Cs, P, Y, Dv, acc_p, acc_v, s, cs, ps, n, h, loop, lane);
+  }
   if constexpr (CERT) {
     __syncwarp();
     if (s <= 16) haf_bound_powers<4, 1>(Ca, M, Ym, Dv, bT, s, cs, ps, n, h, loop, lane);

@@ -272,6 +272,7 @@ static int ws_for_plan(const Plan& P) {
     else if (fn == kFnTor && (tier == kTierDD || tier == kTierCertDD)) w = tor_d_layout(d.dim / 2, tier == kTierCertDD).total;
     else if (fn == kFnTor) w = tor_w_layout(d.dim / 2, tier == kTierCert).total;
     else if (tier == kTierDD || tier == kTierCertDD) w = haf_dd_layout(P.haf_smax, tier == kTierCertDD).total;
+    else if (d.real_in) w = haf_layout(P.haf_smax, tier == kTierCert).total + haf_real_layout(P.haf_smax).total;
     else w = haf_layout(P.haf_smax, tier == kTierCert).total;
     ws = std::max(ws, w);
   }
@@ -366,6 +367,18 @@ static cudaError_t grow_pin(PinBuf& b, size_t bytes) {
 
 // Validate + normalise one request.  Returns 0 or an error code; on success fills
 // the evaluated side length (odd loop hafnian augmented) and the real-input flag.
+// A hafnian or loop hafnian given as host data with every imaginary part zero runs
+// the real power loop in the binary64 tiers (fp64, indicator, certified; the
+// double-double walks are complex only).  Resident-state requests stay complex.
+static bool haf_real_path(const Req& r) {
+  if (r.state || !r.mat) return false;
+  if (r.tier != kTierFp64 && r.tier != kTierKappa && r.tier != kTierCert) return false;
+  const size_t nn = (size_t)r.dim * r.dim;
+  for (size_t i = 0; i < nn; ++i)
+    if (r.mat[2 * i + 1] != 0.0) return false;
+  return true;
+}
+
 static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, cplx* tval) {
   *trivial = false;
   *real_in = false;
@@ -383,12 +396,14 @@ static int check_req(const Req& r, int* dim_eval, bool* real_in, bool* trivial, 
       if (r.dim & 1) { *trivial = true; *tval = mkc(0, 0); return 0; }
       if (r.dim > kHafCap) return fail(cudaErrorInvalidValue, "hafnian: N above the cap 32");
       *dim_eval = r.dim;
+      *real_in = haf_real_path(r);
       return 0;
     case kFnLhaf: {
       if (r.dim == 0) { *trivial = true; *tval = mkc(1, 0); return 0; }
       int d = r.dim + (r.dim & 1);  // lhaf(A) = lhaf(A (+) [1]) for odd N
       if (d > kHafCap) return fail(cudaErrorInvalidValue, "loop hafnian: N above the cap 32");
       *dim_eval = d;
+      *real_in = haf_real_path(r);
       return 0;
     }
     case kFnTor: {

@@ -130,6 +130,55 @@ def test_lhaf_vs_binary128_oracle(gpu, orc, N):
             assert rel_err(got[i], orc.lhaf(mats[i], "quad")) < tol, (N, prec, i)
 
 
+@pytest.mark.parametrize("N", [2, 4, 5, 6, 8, 9, 10, 12, 14, 16, 18, 20])
+def test_real_inputs_vs_binary128_oracle(gpu, orc, N):
+    """A real matrix (every imaginary part zero) runs the real power loop (real
+    m16n8k8 products, K = s): hafnian (even N) and loop hafnian (odd N augmented)
+    against binary128, in fp64 and in the indicator and certified tiers, whose
+    values are the fp64 value bit for bit and whose radius encloses the truth."""
+    U = 2.0 ** -53
+    mats = np.stack([sym(N, cplx=False) for _ in range(3)]).astype(np.complex128)
+    funcs = ["lhaf"] if N % 2 else ["haf", "lhaf"]
+    for f in funcs:
+        fp = _batched(gpu, f)(mats, precision="fp64")
+        vk, dk = _batched(gpu, f)(mats, precision="auto", return_diagnostics=True)
+        vc, dc = _batched(gpu, f)(mats, precision="certified", return_diagnostics=True)
+        for i in range(3):
+            t = getattr(orc, f)(mats[i], "quad")
+            assert np.imag(fp[i]) == 0.0, (f, N, i)
+            assert rel_err(fp[i], t) < FP64_TOL, (f, N, i, fp[i], t)
+            if dk[i]["tier"] == "fp64":
+                assert vk[i] == fp[i], (f, N, i)
+            assert vc[i] == fp[i], (f, N, i)
+            assert abs(vc[i] - t) <= dc[i]["abs_error_bound"] * (1 + 1e-12) + U * abs(t), (f, N, i)
+
+
+@pytest.mark.parametrize("N", [24, 28])
+def test_real_inputs_two_strips_vs_oracle_port(gpu, orc, N):
+    """Real inputs above 16 (two 16-row strips): against the binary64 oracle port
+    of the reference walk, within max(1e-10, 16 N u kappa)."""
+    U = 2.0 ** -53
+    mats = np.stack([sym(N, cplx=False) for _ in range(2)]).astype(np.complex128)
+    for f in ("haf", "lhaf"):
+        got = _batched(gpu, f)(mats, precision="fp64")
+        for i in range(2):
+            v, absn = getattr(orc, f)(mats[i], "fp64", with_absnorm=True)
+            tol = max(1e-10, 16 * N * U * absn / abs(v))
+            assert rel_err(got[i], v) < tol, (f, N, i, got[i], v, absn / abs(v))
+
+
+def test_real_and_complex_mixed_equal_alone(gpu):
+    """Real and complex instances in one persistent launch: each value bit-identical
+    to its evaluation alone (the path is chosen per instance)."""
+    mats = [sym(12, cplx=False).astype(complex), sym(12), sym(20, cplx=False).astype(complex), sym(9, cplx=False),
+            sym(16), sym(26, cplx=False).astype(complex)]
+    funcs = ["haf", "haf", "lhaf", "lhaf", "lhaf", "haf"]
+    with gpu.Workspace() as ws:
+        together = ws.evaluate(funcs, mats, ["fp64"] * len(mats))
+    for i, (f, m) in enumerate(zip(funcs, mats)):
+        assert together[i] == _batched(gpu, f)(np.asarray(m, dtype=complex)[None], precision="fp64")[0], i
+
+
 @pytest.mark.parametrize("n", [13, 16])
 def test_perm_vs_binary128_oracle(gpu, orc, n):
     mats = RNG.standard_normal((2, n, n)) + 1j * RNG.standard_normal((2, n, n))
