@@ -795,39 +795,39 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   if constexpr (REAL) {
     tiny_halving = haf_stage_real<CERT>(A, N, s, loop, gi, Lw.smax, ws, ws + Lw.total, lane);
   } else {
-  const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
-  // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
-  const int dr = 32 / ccols, dc = 32 - dr * ccols;  // (r, c) advance per 32 elements
-  int r = lane / ccols, c = lane - (lane / ccols) * ccols;
-  for (int e = lane; e < rows * ccols; e += 32, r += dr, c += dc) {
-    if (c >= ccols) {
-      c -= ccols;
-      ++r;
-    }
-    cplx v = mkc(0.0, 0.0);
-    if (c < s && r < s) {
-      const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
-      if (loop || rr != cc) {
-        // the symmetric part (A + A^T)/2, exact for a symmetric A: the half-power
-        // identities need B_S symmetric, and the reference's n-1 products of the
-        // raw entries agree with those of the symmetric part to second order in
-        // the antisymmetric part
-        const cplx x = ld_c(A + ((size_t)rr * N + cc) * 2), y = ld_c(A + ((size_t)cc * N + rr) * 2);
-        v = cscale(cadd(x, y), 0.5);
-        if constexpr (CERT) {
-          // halving a sum below twice the smallest normal can round absolutely: no
-          // certificate for such an entry (the relative input bound would not hold)
-          const cplx w = cadd(x, y);
-          if ((x.re != y.re || x.im != y.im) && fmin(fabs(w.re) > 0.0 ? fabs(w.re) : 1.0,
-                                                     fabs(w.im) > 0.0 ? fabs(w.im) : 1.0) < 4.450147717014403e-308)
-            tiny_halving = true;
+    const int ccols = (((2 * s + 7) >> 3) << 2);  // columns read by the n-tiles (>= s)
+    // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
+    const int dr = 32 / ccols, dc = 32 - dr * ccols;  // (r, c) advance per 32 elements
+    int r = lane / ccols, c = lane - (lane / ccols) * ccols;
+    for (int e = lane; e < rows * ccols; e += 32, r += dr, c += dc) {
+      if (c >= ccols) {
+        c -= ccols;
+        ++r;
+      }
+      cplx v = mkc(0.0, 0.0);
+      if (c < s && r < s) {
+        const int rr = gi[r], cc = gi[c ^ 1];  // X swaps the columns within each pair
+        if (loop || rr != cc) {
+          // the symmetric part (A + A^T)/2, exact for a symmetric A: the half-power
+          // identities need B_S symmetric, and the reference's n-1 products of the
+          // raw entries agree with those of the symmetric part to second order in
+          // the antisymmetric part
+          const cplx x = ld_c(A + ((size_t)rr * N + cc) * 2), y = ld_c(A + ((size_t)cc * N + rr) * 2);
+          v = cscale(cadd(x, y), 0.5);
+          if constexpr (CERT) {
+            // halving a sum below twice the smallest normal can round absolutely: no
+            // certificate for such an entry (the relative input bound would not hold)
+            const cplx w = cadd(x, y);
+            if ((x.re != y.re || x.im != y.im) && fmin(fabs(w.re) > 0.0 ? fabs(w.re) : 1.0,
+                                                       fabs(w.im) > 0.0 ? fabs(w.im) : 1.0) < 4.450147717014403e-308)
+              tiny_halving = true;
+          }
         }
       }
+      st_c(Cs + (r * cs + c) * 2, v);
+      if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
     }
-    st_c(Cs + (r * cs + c) * 2, v);
-    if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
-  }
-  if (loop && lane < s) st_c(Dv + lane * 2, ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2));
+    if (loop && lane < s) st_c(Dv + lane * 2, ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2));
   }
   for (int k = lane; k <= n; k += 32) {
     st_c(acc_p + 2 * k, mkc(0.0, 0.0));
