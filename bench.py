@@ -15,7 +15,7 @@ weights gamma ~ CN(0, 0.1) on the loop-hafnian diagonals (gbskernels_b200.worklo
   roofline reference-algorithm FP64 flops of the batch / kernel time, against the
            FP64 tensor-core peak measured live by gbs_probe_fp64_peak
   cpu_baseline    the oracle (binary64 restatement of the reference algorithm) on the
-           host cores, stratified sample: one haf + one lhaf instance per size class
+           host cores, stratified sample: three haf + three lhaf instances per size class
   plain_per_size_sync  the reference's plain per-size path (gbskernels/__init__.py:
            813-852 over core/host_api.cu:537-590): one synchronous session call per
            (function, size) bucket -- stack, H2D, launch, D2H, sync -- and a host
@@ -25,7 +25,7 @@ weights gamma ~ CN(0, 0.1) on the loop-hafnian diagonals (gbskernels_b200.worklo
   configs  the other benchmark configurations, each on its own batch: real 16 x 16
            hafnians (fp64, certified), Haar 20 x 20 permanents (fp64, dd), threshold
            torontonians at 10..24 modes (fp64, certified), with parity spot checks
-  serving  the chain-rule query stream from resident states at 0.75 x and 3 x the
+  serving  the chain-rule query stream from resident states at 0.8 x and 3 x the
            offline rate (the second saturates: its throughput is the capacity)
   check    one haf + one lhaf instance per size class 8..28 of this batch against
            the binary128 oracle (N <= 20) or the binary64 oracle port scaled by the
@@ -631,7 +631,7 @@ def main():
     if not a.no_serving and dist.world == 1:
         from gbskernels_b200.serving import offline_rate, serve_stream
         off = offline_rate(2000, 5)
-        line["serving"] = serve_stream(rate=None, rate_frac=0.75, n_req=2000, seed=5, offline=off)
+        line["serving"] = serve_stream(rate=None, rate_frac=0.8, n_req=2000, seed=5, offline=off)
         line["serving_saturated"] = serve_stream(rate=None, rate_frac=3.0, n_req=2000, seed=5, offline=off)
 
     if dist.rank == 0:

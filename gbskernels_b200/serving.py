@@ -1,6 +1,6 @@
 """Continuous-batching server for chain-rule sampler queries (libgbs_b200 gbs_server_*).
 
-    with Server(slots=4) as srv:
+    with Server(slots=2) as srv:
         st = srv.add_state(A, gamma)                      # resident on the device
         t = srv.submit_state("lhaf", st, idx, "auto", use_gamma=True)
         value, diag = srv.result(t)                       # blocks (bounded) until done
@@ -9,6 +9,12 @@ The scheduler runs in the library (a C++ thread): requests that arrive while
 batches are on the GPU are admitted into the next free slot, up to a workspace
 budget per batch, and up to `slots` batches overlap on the device.  A value is
 independent of the batch it ran in.
+
+Two slots by default: on the chain-rule stream (2000 requests, one B200) two, three,
+four and six slots serve the same throughput below capacity, and two give the
+lowest p99 there (104-117 ms at 0.75x the offline rate, against 128-141 ms with
+four) and the highest saturated throughput (0.89 of offline against 0.88); eight
+lose throughput.
 """
 
 from __future__ import annotations
@@ -54,7 +60,7 @@ def _l():
 class Server:
     """Serving session: `slots` concurrent batches, `budget_bytes` per batch."""
 
-    def __init__(self, slots: int = 4, budget_bytes: int = 256 << 20, max_batch: int = 4096):
+    def __init__(self, slots: int = 2, budget_bytes: int = 256 << 20, max_batch: int = 4096):
         self._lib = _l()
         h = _vp()
         _lib.check(self._lib.gbs_server_open(slots, budget_bytes, max_batch, ctypes.byref(h)), "gbs_server_open")
@@ -166,7 +172,7 @@ def offline_rate(n_req: int = 2000, seed: int = 5):
 
 
 def serve_stream(rate: float | None = None, n_req: int = 2000, seed: int = 5, rate_frac: float = 0.7,
-                 slots: int = 4, budget_bytes: int = 64 << 20, offline=None, resident: bool = True):
+                 slots: int = 2, budget_bytes: int = 64 << 20, offline=None, resident: bool = True):
     """Replay a Poisson stream of chain-rule sampler queries (haf / lhaf / tor,
     matrix side 6..30, growing prefixes per chain, fp64 70% / auto 20% / certified
     10%; workloads.serving_chains) against a Server.
