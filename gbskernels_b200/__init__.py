@@ -542,6 +542,10 @@ def _pack(mats: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
 
 
 _C128 = np.dtype(np.complex128)
+try:  # the batch walk in C (built beside the library); the Python loop below otherwise
+    from . import _hostptr
+except ImportError:
+    _hostptr = None
 
 
 def _pointers(mats) -> tuple[np.ndarray, np.ndarray, list]:
@@ -553,7 +557,9 @@ def _pointers(mats) -> tuple[np.ndarray, np.ndarray, list]:
     ptr = np.empty(B, dtype=np.uint64)
     dims = np.empty(B, dtype=np.int32)
     keep = []
-    for i, m in enumerate(mats):
+    todo = _hostptr.collect(mats, ptr, dims) if _hostptr is not None else range(B)
+    for i in todo:
+        m = mats[i]
         if not (type(m) is np.ndarray and m.dtype == _C128 and m.flags.c_contiguous):
             m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128))
             keep.append(m)

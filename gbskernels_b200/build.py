@@ -68,6 +68,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         for res in ex.map(compile_one, zip(srcs, objs)):
             if res and verbose:
                 print(f"[build] {res[0]}", res[1][-2000:], file=sys.stderr)
+    build_host_helper()
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
@@ -75,6 +76,26 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
     return LIB
+
+
+def build_host_helper() -> Path | None:
+    """The CPython helper of the binding (_hostptr.c: matrix addresses of a batch in
+    one C loop), compiled with the host C compiler.  Optional: without it the
+    binding walks the batch in Python."""
+    import sysconfig
+    src = HERE / "_hostptr.c"
+    out = HERE / ("_hostptr" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+    inc = sysconfig.get_paths().get("include")
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc or not inc or not (Path(inc) / "Python.h").exists():
+        return None
+    if out.exists() and out.stat().st_mtime >= src.stat().st_mtime:
+        return out
+    r = subprocess.run([cc, "-O2", "-shared", "-fPIC", "-I", inc, str(src), "-o", str(out)],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building {src.name} failed:\n{r.stderr[-4000:]}")
+    return out
 
 
 if __name__ == "__main__":
