@@ -24,9 +24,11 @@ weights gamma ~ CN(0, 0.1) on the loop-hafnian diagonals (gbskernels_b200.worklo
            instances of the same mix (where one launch per size underfills the GPU)
   configs  the other benchmark configurations, each on its own batch: real 16 x 16
            hafnians (fp64, certified), Haar 20 x 20 permanents (fp64, dd), threshold
-           torontonians at 10..24 modes (fp64, certified), with parity spot checks
+           torontonians at 10..24 modes (fp64, certified), with parity spot checks;
+           the repeated-row sieve and the resident sampler chain (host-call rates)
   serving  the chain-rule query stream from resident states at 0.8 x and 3 x the
-           offline rate (the second saturates: its throughput is the capacity)
+           offline rate (the second saturates: its throughput is the capacity), and
+           at the configuration's arrival rates 1e3 .. 1e5 requests/s
   check    one haf + one lhaf instance per size class 8..28 of this batch against
            the binary128 oracle (N <= 20) or the binary64 oracle port scaled by the
            instance's cancellation indicator (N >= 22)
@@ -429,6 +431,9 @@ def other_configs(G, peak, cores):
             "instances": len(lst), "max_rel_err": float(max(x["rel_err"] for x in lst)),
             "certified_enclose": all(x.get("certified_encloses", True) for x in lst),
             "max_dd_rel_err": max((float(x["dd_rel_err"]) for x in lst if "dd_rel_err" in x), default=None)}
+    # beside the power-trace path: the repeated-row sieve and the resident sampler chain
+    out["sieve_lhaf_repeated"] = configs.sieve_rate()
+    out["sampler_chain"] = configs.sampler_rate()
     return out
 
 # ---------------------------------------------------------------- our implementation
@@ -633,6 +638,12 @@ def main():
         off = offline_rate(2000, 5)
         line["serving"] = serve_stream(rate=None, rate_frac=0.8, n_req=2000, seed=5, offline=off)
         line["serving_saturated"] = serve_stream(rate=None, rate_frac=3.0, n_req=2000, seed=5, offline=off)
+        # the configuration's own arrival rates (Poisson, 2000 requests each)
+        keep = ("offered_rate", "throughput", "throughput_vs_offline", "p50_ms", "p99_ms", "batches",
+                "values_equal_to_offline_batch")
+        line["serving_rate_sweep"] = [
+            {k: r[k] for k in keep} for r in
+            (serve_stream(rate=lam, n_req=2000, seed=5, offline=off) for lam in (1e3, 3e3, 1e4, 3e4, 1e5))]
 
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
