@@ -17,7 +17,10 @@
 // host-to-device copy is involved, so nothing the call leaves behind on the host
 // can be read by the GPU later.
 //
-// The result equals gbs_haf_host's bit for bit (same work items, same kernel).
+// The result equals gbs_haf_host's bit for bit for complex input (same work items,
+// same kernel).  Every input here takes the complex power loop; gbs_haf_host runs
+// a real input (every imaginary part zero) through the real loop, so for real
+// input the two agree to rounding.
 #include <cuda_runtime.h>
 
 #include <cstdio>

@@ -271,7 +271,10 @@ int gbs_server_stats(gbs_server* sv, long long* completed, long long* batches, l
  * kernel, so no host buffer is read after the call returns.  The first call on a
  * device looks up the array's address (make it before any stream capture); calls
  * that overlap on the GPU share the array and race.  Asynchronous on `stream` (a
- * cudaStream_t).  Values equal gbs_haf_host's bit for bit (same split).         */
+ * cudaStream_t).  Values equal gbs_haf_host's bit for bit for complex input
+ * (same split, same kernel).  Every input here runs the complex power loop: for a
+ * real input (every imaginary part zero) gbs_haf_host runs the real one instead,
+ * and the two then agree to rounding, not bit for bit.                          */
 int gbs_haf_noalloc(const double* d_mats, int N, int batch, double* d_out, void* stream);
 const char* gbs_haf_noalloc_last_error(void);
 

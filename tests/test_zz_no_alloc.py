@@ -72,6 +72,18 @@ def test_noalloc_matches_host_entry_point_twice(lib):
         assert np.array_equal(got, ref)
 
 
+def test_noalloc_real_input_agrees_to_rounding(lib):
+    # a real input runs the real power loop through gbs_haf_host and the complex one
+    # here: equal to rounding, not bit for bit
+    rng = np.random.default_rng(31)
+    for N in (12, 20):
+        stack = np.ascontiguousarray(_sym(rng, 16, N).real.astype(np.complex128))
+        got = _haf_noalloc(lib, stack)
+        ref = _haf_host(lib, stack)
+        assert np.all(np.isfinite(got))
+        assert np.allclose(got, ref, rtol=1e-10, atol=0.0), (N, np.max(np.abs(got - ref) / np.abs(ref)))
+
+
 def test_noalloc_trivial_sides(lib):
     rng = np.random.default_rng(7)
     # N = 0: haf = 1; odd N: haf = 0 -- written by the library, not left over
