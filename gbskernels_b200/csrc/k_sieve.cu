@@ -355,6 +355,31 @@ using namespace gbsb;
 
 namespace {
 // Plain (bound == nullptr) or certified evaluation of a batch of patterns.
+// Device buffers of the sieve, kept per device between calls and grown only when a
+// call needs more (the tables are uploaded once per device).  Allocating and
+// freeing them per call cost more host time than the sieve kernels of a
+// 4096-pattern batch (cudaFree synchronises the device).  Calls hold g_sieve_mu.
+struct SieveBufs {
+  double *A = nullptr, *g = nullptr, *coef = nullptr, *bin = nullptr, *part = nullptr, *out = nullptr,
+         *part_r = nullptr, *out_r = nullptr;
+  SievePattern* pats = nullptr;
+  size_t cap_A = 0, cap_g = 0, cap_part = 0, cap_out = 0, cap_pats = 0, cap_part_r = 0, cap_out_r = 0;
+};
+constexpr int kSieveDevs = 64;
+SieveBufs g_sieve[kSieveDevs];
+std::mutex g_sieve_mu;
+
+template <typename T>
+cudaError_t sieve_grow(T** p, size_t* cap, size_t n) {
+  if (n <= *cap) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const cudaError_t e = cudaMalloc(p, sizeof(T) * n);
+  if (e == cudaSuccess) *cap = n;
+  return e;
+}
+
 int sieve_run(const double* A_in, const double* gamma, int M, const int* reps, int batch, double* out,
               double* bound) {
   const bool cert = bound != nullptr;
@@ -433,31 +458,45 @@ int sieve_run(const double* A_in, const double* gamma, int M, const int* reps, i
     }
     pats[p] = P;
   }
-  double *dA = nullptr, *dg = nullptr, *dcoef = nullptr, *dbin = nullptr, *dpart = nullptr, *dout = nullptr;
-  double *dpart_r = nullptr, *dout_r = nullptr;
-  SievePattern* dpats = nullptr;
   std::vector<double> g0;
   if (!gamma) {
     g0.assign(2 * (size_t)std::max(M, 1), 0.0);
     gamma = g0.data();
   }
-  cudaError_t e = cudaMalloc(&dA, sizeof(double) * 2 * std::max(M * M, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&dg, sizeof(double) * 2 * std::max(M, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&dcoef, sizeof(double) * T.coef.size());
-  if (e == cudaSuccess) e = cudaMalloc(&dbin, sizeof(double) * T.binom.size());
-  if (e == cudaSuccess) e = cudaMalloc(&dpart, sizeof(double) * 2 * std::max(items, 1ll));
-  if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * 2 * batch);
-  if (e == cudaSuccess) e = cudaMalloc(&dpats, sizeof(SievePattern) * batch);
-  if (e == cudaSuccess && cert) e = cudaMalloc(&dpart_r, sizeof(double) * std::max(items, 1ll));
-  if (e == cudaSuccess && cert) e = cudaMalloc(&dout_r, sizeof(double) * batch);
+  std::lock_guard<std::mutex> lk(g_sieve_mu);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kSieveDevs)
+    return sieve_fail(e != cudaSuccess ? (int)e : (int)cudaErrorInvalidDevice, "lhaf_repeated: no usable device");
+  SieveBufs& Bf = g_sieve[dev];
+  if (!Bf.coef) {  // the tables, once per device
+    e = cudaMalloc(&Bf.coef, sizeof(double) * T.coef.size());
+    if (e == cudaSuccess) e = cudaMalloc(&Bf.bin, sizeof(double) * T.binom.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(Bf.coef, T.coef.data(), sizeof(double) * T.coef.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(Bf.bin, T.binom.data(), sizeof(double) * T.binom.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      if (Bf.coef) cudaFree(Bf.coef);
+      if (Bf.bin) cudaFree(Bf.bin);
+      Bf.coef = Bf.bin = nullptr;
+    }
+  }
+  if (e == cudaSuccess) e = sieve_grow(&Bf.A, &Bf.cap_A, 2 * (size_t)std::max(M * M, 1));
+  if (e == cudaSuccess) e = sieve_grow(&Bf.g, &Bf.cap_g, 2 * (size_t)std::max(M, 1));
+  if (e == cudaSuccess) e = sieve_grow(&Bf.part, &Bf.cap_part, 2 * (size_t)std::max(items, 1ll));
+  if (e == cudaSuccess) e = sieve_grow(&Bf.out, &Bf.cap_out, 2 * (size_t)batch);
+  if (e == cudaSuccess) e = sieve_grow(&Bf.pats, &Bf.cap_pats, (size_t)batch);
+  if (e == cudaSuccess && cert) e = sieve_grow(&Bf.part_r, &Bf.cap_part_r, (size_t)std::max(items, 1ll));
+  if (e == cudaSuccess && cert) e = sieve_grow(&Bf.out_r, &Bf.cap_out_r, (size_t)batch);
+  double *dA = Bf.A, *dg = Bf.g, *dcoef = Bf.coef, *dbin = Bf.bin, *dpart = Bf.part, *dout = Bf.out;
+  double *dpart_r = cert ? Bf.part_r : nullptr, *dout_r = cert ? Bf.out_r : nullptr;
+  SievePattern* dpats = Bf.pats;
   if (e == cudaSuccess && M > 0) e = cudaMemcpy(dA, A, sizeof(double) * 2 * M * M, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && M > 0) e = cudaMemcpy(dg, gamma, sizeof(double) * 2 * M, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(dcoef, T.coef.data(), sizeof(double) * T.coef.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(dbin, T.binom.data(), sizeof(double) * T.binom.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dpats, pats.data(), sizeof(SievePattern) * batch, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && items > 0) {
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
+    int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long want = (items + 3) / 4;
     const int grid = (int)std::max(1ll, std::min<long long>(want, (long long)sms * 16));
@@ -472,9 +511,6 @@ int sieve_run(const double* A_in, const double* gamma, int M, const int* reps, i
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && cert) e = cudaMemcpy(bound, dout_r, sizeof(double) * batch, cudaMemcpyDeviceToHost);
-  for (void* p : {(void*)dA, (void*)dg, (void*)dcoef, (void*)dbin, (void*)dpart, (void*)dout, (void*)dpats,
-                  (void*)dpart_r, (void*)dout_r})
-    if (p) cudaFree(p);
   if (e != cudaSuccess) return sieve_fail((int)e, std::string("lhaf_repeated: ") + cudaGetErrorString(e));
   if (cert)
     for (int p = 0; p < batch; ++p) {
