@@ -209,19 +209,25 @@ __device__ __forceinline__ bool tor_d_append(const double* __restrict__ Oc, int 
   return ok;
 }
 
-// One prefix leaf: lanes 0..2^r-1 factor their tail subset; returns the signed term.
-__device__ __forceinline__ dd tor_d_leaf(const double* zc, const double* zid, int r, int c, int k, dd detc, int lane,
-                                         bool& ok, int& m) {
+// Two prefix leaves at once: the half warp h (lane >> 4) factors the tail subsets
+// (lane & 15 < 2^r) of the leaf at depth c[h] (Schur complement zc[h], determinant
+// detc[h]); with two == false only the first half works.  Returns the signed term.
+__device__ __forceinline__ dd tor_d_leaf(const double* zc0, const double* zc1, const double* zid, int r, int c0,
+                                         int c1, int k, dd det0, dd det1, bool two, int lane, bool& ok, int& m) {
   dd term = dd_make(0.0);
   m = 0;
-  if (lane < (1 << r)) {
+  const int half = lane >> 4, sub = lane & 15;
+  if ((two || half == 0) && sub < (1 << r)) {
+    const double* zc = half ? zc1 : zc0;
+    const int c = half ? c1 : c0;
+    const dd detc = half ? det1 : det0;
     const int td = 2 * r;
     dd Lz[kTorZEdd];
     dd iv[kTorTDdd];
     dd det = dd_make(1.0);
 #pragma unroll
     for (int i = 0; i < kTorTDdd; ++i) {
-      const bool in_i = i < td && ((lane >> (i >> 1)) & 1);
+      const bool in_i = i < td && ((sub >> (i >> 1)) & 1);
       const double* zr = (in_i ? zc : zid) + 2 * (i * (i + 1) / 2);
 #pragma unroll
       for (int jj = 0; jj <= i; ++jj) {
@@ -241,7 +247,7 @@ __device__ __forceinline__ dd tor_d_leaf(const double* zc, const double* zid, in
         }
       }
     }
-    const int nin = __popc(lane);
+    const int nin = __popc(sub);
     m = 2 * (c + nin);
     const dd t = dd_rsqrt(dd_mul(detc, det));
     term = ((k - c - nin) & 1) ? dd_neg(t) : t;
@@ -325,8 +331,16 @@ static __device__ bool tor_dd_item(const double* __restrict__ Oc, int k, int g, 
   double srad = 0.0;
   constexpr double kU2x4 = 4.0 * kU * kU;  // bound of one dd_add, relative, with slack
   const int rp = q - g;
-  const uint64_t nT = 1ull << rp;
-  for (uint64_t Tm = 0; Tm < nT; ++Tm) {
+  // The walked modes [g, q) in binary-counter order, the last one (q - 1) as the
+  // lowest bit: the leaves come in sibling pairs (q - 1 out, then in).  After the
+  // append of q - 1 both siblings' Schur complements and determinants are in shared
+  // memory (depths c and c + 1), so one pass factors both, a half warp each (the
+  // 16 tail subsets of a leaf fill only half the lanes).  Each term is the one the
+  // leaf gives alone; the sum takes them in another order.
+  const bool pairs = rp > 0 && r == kTorTailDD;
+  const uint64_t nT = 1ull << (pairs ? rp - 1 : rp);
+  for (uint64_t Tp = 0; Tp < nT; ++Tp) {
+    const uint64_t Tm = pairs ? 2 * Tp : Tp;
     if (Tm) {
       const int z = __ffsll((long long)Tm) - 1;
       const int jz = g + rp - 1 - z;
@@ -334,8 +348,10 @@ static __device__ bool tor_dd_item(const double* __restrict__ Oc, int k, int g, 
       ok = tor_d_append(Oc, k, q, r, jz, count, col, inv, zd, detat, gidx, lane, zi, zj) && ok;
       ++count;
     }
+    if (pairs) ok = tor_d_append(Oc, k, q, r, q - 1, count, col, inv, zd, detat, gidx, lane, zi, zj) && ok;
     int m = 0;
-    const dd t = tor_d_leaf(zd + 2 * count * kTorZEdd, zid, r, count, k, ld_dd(detat + 2 * count), lane, ok, m);
+    const dd t = tor_d_leaf(zd + 2 * count * kTorZEdd, zd + 2 * (count + 1) * kTorZEdd, zid, r, count, count + 1, k,
+                            ld_dd(detat + 2 * count), ld_dd(detat + 2 * (count + 1)), pairs, lane, ok, m);
     if (CERT) {
       // ball butterfly: the value operations are those of warp_sum_dd
       dd v = t;
