@@ -78,6 +78,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "gbs_sampler_conditional_weights": ([_dp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int,
                                          ctypes.c_int, _dp], ctypes.c_int),
     "gbs_sampler_last_error": ([], ctypes.c_char_p),
+    "gbs_sampler_set_dedup": ([ctypes.c_int], ctypes.c_int),
     "gbs_lhaf_repeated_last_error": ([], ctypes.c_char_p),
     "gbs_probe_fp64_peak": ([_dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "gbs_probe_fp64_mma": ([ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),

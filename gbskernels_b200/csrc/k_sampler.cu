@@ -30,13 +30,20 @@ constexpr int kSamplerMaxN = 32;  // the hafnian path's cap (2 M cutoff <= 32)
 //   [mode i x prefix[i]] + [mode k-1 x j] + [mode i+k x prefix[i]] + [mode 2k-1 x j],
 // and the compact n x n submatrix A_k[idx, idx] at the slot of the instance, with the
 // instance's descriptor (its work items are assigned by sampler_plan_kernel).
+// With `urep` (the prefixes deduplicated, see sampler_key_kernel): instance t is
+// candidate j of unique prefix t / (cutoff + 1), read from its representative draw
+// urep[u]; instances past *nuniq x (cutoff + 1) are not written.
 __global__ void __launch_bounds__(128) sampler_gather_kernel(const double* __restrict__ Ak, int k,
                                                              const int* __restrict__ state, int M, int d0,
                                                              int ndraw, int cutoff, int slot, double* __restrict__ sub,
-                                                             InstDesc* __restrict__ insts, int* __restrict__ overflow) {
+                                                             InstDesc* __restrict__ insts, int* __restrict__ overflow,
+                                                             const int* __restrict__ urep,
+                                                             const int* __restrict__ nuniq) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ndraw * (cutoff + 1)) return;
-  const int d = d0 + t / (cutoff + 1), j = t % (cutoff + 1);
+  const int u = t / (cutoff + 1), j = t % (cutoff + 1);
+  if (urep && u >= *nuniq) return;
+  const int d = urep ? urep[u] : d0 + u;
   const int* pre = state + (size_t)d * M;
   const int twok = 2 * k;
   int idx[kSamplerMaxN];
@@ -87,9 +94,11 @@ __global__ void __launch_bounds__(128) sampler_gather_kernel(const double* __res
 constexpr int kSamplerPlanThreads = 1024;
 __global__ void __launch_bounds__(kSamplerPlanThreads) sampler_plan_kernel(InstDesc* __restrict__ insts, int ni,
                                                                            WorkItem* __restrict__ items,
-                                                                           int* __restrict__ n_items) {
+                                                                           int* __restrict__ n_items,
+                                                                           const int* __restrict__ nuniq, int per_u) {
   __shared__ long long part[kSamplerPlanThreads];
   const int tid = threadIdx.x;
+  if (nuniq) ni = min(ni, *nuniq * per_u);  // deduplicated prefixes: the unique instances only
   const int per = (ni + kSamplerPlanThreads - 1) / kSamplerPlanThreads;
   const int t0 = min(ni, tid * per), t1 = min(ni, t0 + per);
   auto splits = [&](int t) -> long long {
@@ -130,11 +139,14 @@ __global__ void __launch_bounds__(kSamplerPlanThreads) sampler_plan_kernel(InstD
 // one uniform from the draw's stream; the count goes to state[d][k-1].
 __global__ void __launch_bounds__(128) sampler_draw_kernel(const double* __restrict__ haf, const double* __restrict__ invfac,
                                                            int cutoff, int d0, int ndraw, unsigned long long seed, int k,
-                                                           int* __restrict__ state, int M) {
+                                                           int* __restrict__ state, int M,
+                                                           const int* __restrict__ slot_of,
+                                                           const int* __restrict__ sid) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ndraw) return;
   const int d = d0 + t;
-  const double* w = haf + (size_t)t * (cutoff + 1) * 2;  // complex values, real parts used
+  const int u = slot_of ? sid[slot_of[t]] : t;  // the draw's (unique) prefix
+  const double* w = haf + (size_t)u * (cutoff + 1) * 2;  // complex values, real parts used
   double sum = 0.0;
   for (int j = 0; j <= cutoff; ++j) sum += fmax(w[2 * j], 0.0) * invfac[j];
   int photon = 0;
@@ -152,6 +164,90 @@ __global__ void __launch_bounds__(128) sampler_draw_kernel(const double* __restr
   state[(size_t)d * M + (k - 1)] = photon;
 }
 
+// ---- prefix deduplication.  The conditional hafnians of mode k depend on a draw
+// only through its prefix (the counts of modes 1..k-1), and with few photons many
+// of the draws share one: at M = 8 and cutoff 2 there are at most 3^7 = 2187
+// prefixes at the last mode against 10^5 draws.  Each prefix is a mixed-radix key
+// (radix cutoff + 1, used only when (cutoff + 1)^(M - 1) < 2^62), inserted into an
+// open-addressing table (linear probing, at least twice as many slots as draws);
+// the occupied slots are numbered by one scan, and every unique prefix is gathered
+// and evaluated once.  A hafnian does not depend on which instance slot holds it,
+// so the draws are bit-identical to evaluating every draw's conditionals.
+constexpr unsigned long long kSamplerEmpty = ~0ull;
+
+__device__ __forceinline__ unsigned long long sampler_mix(unsigned long long x) {
+  // SplitMix64 finaliser (Steele, Lea, Flood 2014): spreads nearby keys over the table
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
+
+// One thread per draw: insert the prefix key; record the draw's table slot and, for
+// the first draw of a key, that draw as the key's representative.  The probe visits
+// each slot at most once (the table has more slots than draws, so it always ends).
+__global__ void __launch_bounds__(128) sampler_key_kernel(const int* __restrict__ state, int M, int d0, int ndraw,
+                                                          int k, int radix, unsigned long long* __restrict__ tkeys,
+                                                          int* __restrict__ trep, int tmask,
+                                                          int* __restrict__ slot_of) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ndraw) return;
+  const int d = d0 + t;
+  const int* pre = state + (size_t)d * M;
+  unsigned long long key = 0, mul = 1;
+  for (int i = 0; i < k - 1; ++i) {
+    key += (unsigned long long)pre[i] * mul;
+    mul *= (unsigned long long)radix;
+  }
+  unsigned int h = (unsigned int)(sampler_mix(key) & (unsigned long long)tmask);
+  for (int probe = 0; probe <= tmask; ++probe) {
+    const unsigned long long prev = atomicCAS(tkeys + h, kSamplerEmpty, key);
+    if (prev == kSamplerEmpty) {
+      trep[h] = d;
+      break;
+    }
+    if (prev == key) break;
+    h = (h + 1) & (unsigned int)tmask;
+  }
+  slot_of[t] = (int)h;
+}
+
+// One block: number the occupied slots in slot order (sid[slot], -1 when empty), the
+// representatives urep[id] and the count *nuniq.
+__global__ void __launch_bounds__(kSamplerPlanThreads) sampler_compact_kernel(
+    const unsigned long long* __restrict__ tkeys, const int* __restrict__ trep, int tsize, int* __restrict__ sid,
+    int* __restrict__ urep, int* __restrict__ nuniq) {
+  __shared__ int part[kSamplerPlanThreads];
+  const int tid = threadIdx.x;
+  const int per = (tsize + kSamplerPlanThreads - 1) / kSamplerPlanThreads;
+  const int h0 = min(tsize, tid * per), h1 = min(tsize, h0 + per);
+  int mine = 0;
+  for (int h = h0; h < h1; ++h) mine += tkeys[h] != kSamplerEmpty;
+  part[tid] = mine;
+  __syncthreads();
+  for (int off = 1; off < kSamplerPlanThreads; off <<= 1) {
+    const int v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  int id = part[tid] - mine;
+  for (int h = h0; h < h1; ++h) {
+    if (tkeys[h] != kSamplerEmpty) {
+      sid[h] = id;
+      urep[id] = trep[h];
+      ++id;
+    } else {
+      sid[h] = -1;
+    }
+  }
+  if (tid == kSamplerPlanThreads - 1) *nuniq = part[tid];
+}
+
+bool g_sampler_dedup = true;  // gbs_sampler_set_dedup
+
 namespace {
 thread_local std::string t_sampler_err;
 int sampler_fail(int code, const std::string& msg) {
@@ -165,10 +261,14 @@ struct SamplerBufs {
   int *state = nullptr, *head = nullptr, *done = nullptr, *pst = nullptr, *st = nullptr, *overflow = nullptr;
   InstDesc* insts = nullptr;
   WorkItem* items = nullptr;
+  // prefix deduplication: the table (keys, representative draw, slot number), each
+  // draw's slot, the unique prefixes' representatives and their count
+  unsigned long long* tkeys = nullptr;
+  int *trep = nullptr, *sid = nullptr, *slot_of = nullptr, *urep = nullptr, *nuniq = nullptr;
   ~SamplerBufs() {
     for (void* p : {(void*)Ak, (void*)invfac, (void*)sub, (void*)part, (void*)paux, (void*)out, (void*)aux,
                     (void*)state, (void*)head, (void*)done, (void*)pst, (void*)st, (void*)overflow, (void*)insts,
-                    (void*)items})
+                    (void*)items, (void*)tkeys, (void*)trep, (void*)sid, (void*)slot_of, (void*)urep, (void*)nuniq})
       if (p) cudaFree(p);
   }
 };
@@ -199,11 +299,29 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
   const int slot_max = std::max(2, std::min(kSamplerMaxN, 2 * M * cutoff));
   // work items per instance at most (2^7 subsets each)
   const size_t max_split = (size_t)1 << std::max(0, slot_max / 2 - kHafItemLog2);
-  // draws per chunk: the slots and the item arrays of one step stay within 1 GiB
+  // the slots and item arrays of one step's instances stay within 1 GiB
   const size_t draw_bytes = (size_t)per * ((size_t)slot_max * slot_max * 16 +
                                            max_split * (sizeof(WorkItem) + 4 * sizeof(double) + sizeof(double) + sizeof(int)));
-  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(num_draws, (size_t)(1ull << 30) / draw_bytes));
-  const int ninst = chunk * per;
+  const size_t fit = std::max<size_t>(1, (size_t)(1ull << 30) / draw_bytes);  // prefixes whose instances fit
+  // prefix deduplication when sampling and every prefix key fits: (cutoff + 1)^(M - 1) < 2^62
+  bool dedup = g_sampler_dedup && !weights_out;
+  long double span = 1.0L;  // distinct prefixes at the last mode at most
+  for (int i = 0; i < M - 1 && dedup; ++i) {
+    span *= (long double)per;
+    if (span >= 4.611686018427387904e18L) dedup = false;
+  }
+  // draws per chunk and distinct prefixes per step: without deduplication every draw
+  // has its own instances; with it the instances follow the distinct prefixes, so
+  // when they all fit a chunk can hold up to 2^22 draws (its table and slots alone)
+  int chunk, ucap;
+  if (dedup && span <= (long double)fit) {
+    chunk = (int)std::min<long long>(num_draws, 1ll << 22);
+    ucap = (int)std::min<long double>((long double)chunk, span);
+  } else {
+    chunk = (int)std::min<size_t>(num_draws, fit);
+    ucap = chunk;
+  }
+  const int ninst = ucap * per;
   const size_t nitem_cap = (size_t)ninst * max_split;
   if (nitem_cap > (size_t)INT32_MAX) return sampler_fail((int)cudaErrorInvalidValue, "sampler: too many work items");
   cudaError_t e = cudaMalloc(&B.Ak, sizeof(double) * 2 * std::max<long long>(ak_total, 1));
@@ -221,6 +339,14 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
   if (e == cudaSuccess) e = cudaMalloc(&B.overflow, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&B.insts, sizeof(InstDesc) * ninst);
   if (e == cudaSuccess) e = cudaMalloc(&B.items, sizeof(WorkItem) * nitem_cap);
+  int tsize = 1;
+  while (tsize < 2 * chunk) tsize <<= 1;
+  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.tkeys, sizeof(unsigned long long) * tsize);
+  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.trep, sizeof(int) * tsize);
+  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.sid, sizeof(int) * tsize);
+  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.slot_of, sizeof(int) * chunk);
+  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.urep, sizeof(int) * chunk);
+  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.nuniq, sizeof(int));
   if (e != cudaSuccess) return sampler_fail((int)e, "sampler: device allocation failed");
   cudaStream_t s = nullptr;
   e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -268,15 +394,30 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
     const int ni = nd * per;
     for (int k = kfirst; k <= kmax && e == cudaSuccess; ++k) {
       const int slot = std::max(2, std::min(kSamplerMaxN, 2 * k * cutoff));
+      if (dedup) {
+        e = cudaMemsetAsync(B.tkeys, 0xFF, sizeof(unsigned long long) * tsize, s);
+        if (e == cudaSuccess) {
+          sampler_key_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.state, M, d0, nd, k, per, B.tkeys, B.trep, tsize - 1,
+                                                              B.slot_of);
+          e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) {
+          sampler_compact_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.tkeys, B.trep, tsize, B.sid, B.urep, B.nuniq);
+          e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) break;
+      }
       sampler_gather_kernel<<<(ni + 127) / 128, 128, 0, s>>>(B.Ak + 2 * (size_t)h_off[k - 1], k, B.state, M, d0, nd,
-                                                            cutoff, slot, B.sub, B.insts, B.overflow);
+                                                            cutoff, slot, B.sub, B.insts, B.overflow,
+                                                            dedup ? B.urep : nullptr, dedup ? B.nuniq : nullptr);
       e = cudaGetLastError();
       if (e == cudaSuccess) {
-        sampler_plan_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.insts, ni, B.items, B.head + 1);
+        sampler_plan_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.insts, ni, B.items, B.head + 1,
+                                                             dedup ? B.nuniq : nullptr, per);
         e = cudaGetLastError();
       }
       if (e == cudaSuccess) e = cudaMemsetAsync(B.head, 0, sizeof(int), s);
-      if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, sizeof(int) * ni, s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, sizeof(int) * std::min(ni, ninst), s);
       if (e == cudaSuccess) {
         L.n_items = (int)nitem_cap;  // upper bound; the kernel reads the planned count
         e = launch_br<BR>(L, sms * bps, 1, s);
@@ -289,7 +430,8 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
         for (int t = 0; t < ni && e == cudaSuccess; ++t) weights_out[(size_t)d0 * per + t] = o[2 * (size_t)t];
         break;
       }
-      sampler_draw_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.out, B.invfac, cutoff, d0, nd, seed, k, B.state, M);
+      sampler_draw_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.out, B.invfac, cutoff, d0, nd, seed, k, B.state, M,
+                                                           dedup ? B.slot_of : nullptr, dedup ? B.sid : nullptr);
       e = cudaGetLastError();
     }
   }
@@ -319,6 +461,14 @@ int gbs_sampler_sample(const double* h_Ak, int ak_total, const int* h_off, int M
                        int maxn, const double* h_invfac, unsigned long long seed, int* h_out) {
   (void)maxn;
   return sampler_chain(h_Ak, ak_total, h_off, M, num_draws, cutoff, h_invfac, seed, h_out, 0, nullptr, nullptr);
+}
+
+// Prefix deduplication of the sampler chain on (1, default) or off (0): every draw's
+// conditional hafnians evaluated separately.  The samples are the same either way;
+// the switch exists to check that.  Process-wide.
+int gbs_sampler_set_dedup(int on) {
+  g_sampler_dedup = on != 0;
+  return 0;
 }
 
 // The conditional weights Re haf(A_k[idx, idx]) of mode k for given prefixes

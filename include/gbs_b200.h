@@ -120,6 +120,8 @@ const char* gbs_lhaf_repeated_last_error(void);
  * gathered on the device, their hafnians evaluated by the work-item kernel and the
  * count drawn by inverse CDF of clip(Re haf, 0) * h_invfac[j] (one Philox4_32_10
  * uniform per draw and mode, subsequence = draw index); h_out: num_draws x M counts.
+ * Draws that share a prefix (the counts of the modes before k) share their
+ * conditional hafnians, which are evaluated once per distinct prefix.
  * Requires 2 M cutoff <= 32 (maxn is accepted for the reference's signature).      */
 int gbs_sampler_sample(const double* h_Ak, int ak_total, const int* h_off, int M, int num_draws, int cutoff,
                        int maxn, const double* h_invfac, unsigned long long seed, int* h_out);
@@ -129,6 +131,10 @@ int gbs_sampler_sample(const double* h_Ak, int ak_total, const int* h_off, int M
 int gbs_sampler_conditional_weights(const double* h_Ak, int ak_total, const int* h_off, int M, int k,
                                     const int* h_state, int num_draws, int cutoff, double* h_w);
 const char* gbs_sampler_last_error(void);
+/* prefix sharing of gbs_sampler_sample on (1, the default) or off (0: every draw's
+ * conditionals evaluated separately); the samples are identical either way.
+ * Process-wide.  No reference counterpart.                                        */
+int gbs_sampler_set_dedup(int on);
 
 /* ---- auto tier on the device ----------------------------------------------
  * reference: gbskernels/__init__.py:272-297 (_gpu_auto_batched) whose fp64 pass is

@@ -95,3 +95,20 @@ def test_seeds_and_edge_cases(gpu):
     assert np.all(sampler.sample_resident(vac, 100, cutoff=4, seed=1) == 0)
     with pytest.raises(ValueError):
         sampler.sample_resident(_cov(5), 10, cutoff=4)  # 2 M cutoff = 40 > 32
+
+
+@pytest.mark.parametrize("M,cutoff,S", [(8, 2, 20000), (4, 4, 20000), (16, 1, 5000), (2, 8, 3000)])
+def test_prefix_sharing_gives_the_same_samples(gpu, lib, M, cutoff, S):
+    """Draws that share a prefix share their conditional hafnians (evaluated once per
+    distinct prefix): the samples equal, count for count, those of evaluating every
+    draw's conditionals separately, with the same seed."""
+    from gbskernels_b200 import sampler
+    cov = _cov(M, seed=5)
+    try:
+        lib.gbs_sampler_set_dedup(0)
+        plain = sampler.sample_resident(cov, S, cutoff=cutoff, seed=21)
+    finally:
+        lib.gbs_sampler_set_dedup(1)
+    shared = sampler.sample_resident(cov, S, cutoff=cutoff, seed=21)
+    assert np.array_equal(shared, plain)
+    assert shared.sum() > 0
