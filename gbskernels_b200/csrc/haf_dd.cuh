@@ -34,6 +34,20 @@ struct HafDDLayout {
   // haf_pt.cuh), row bounds, trace / loop bound sums, d in binary64
   int ca_off, m_off, ym_off, bt_off, dv_off;
 };
+// Row stride (doubles) of the double-word power buffers for a subset of side s: at
+// least the row's 4 s doubles and == 4 (mod 16), so consecutive rows start 32 bytes
+// apart modulo 128 and every complex double word stays 32-byte aligned (ld_ddc is
+// one 32-byte load).  The strip product reads one complex double word of each of
+// the 16 rows at a time: with rows a multiple of 128 bytes long (s a multiple of 4)
+// all 16 fell on the same banks, 16 wavefronts per load; 32 bytes apart they fill
+// each 128-byte wavefront four at a time, the minimum of 4.
+__host__ __device__ inline int haf_dd_prow(int s) { return 4 * s + ((4 - 4 * s) & 15); }
+__host__ __device__ inline int haf_dd_prow_max(int smax) {
+  int m = 0;
+  for (int s = 2; s <= smax; s += 2) m = m > haf_dd_prow(s) ? m : haf_dd_prow(s);
+  return m;
+}
+
 __host__ __device__ inline HafDDLayout haf_dd_layout(int smax, bool cert = false) {
   HafDDLayout L;
   if (smax < 2) smax = 2;
@@ -41,8 +55,8 @@ __host__ __device__ inline HafDDLayout haf_dd_layout(int smax, bool cert = false
   int h = (smax / 2 + 1) / 2;
   L.c_off = 0;
   L.p0_off = L.c_off + smax * smax * 4;
-  L.p1_off = L.p0_off + 16 * smax * 4;
-  L.y_off = L.p1_off + 16 * smax * 4;
+  L.p1_off = L.p0_off + 16 * haf_dd_prow_max(smax);
+  L.y_off = L.p1_off + 16 * haf_dd_prow_max(smax);
   L.d_off = L.y_off + 16 * (h + 1) * 4;
   L.gi_off = L.d_off + 32 * 4;
   L.acc_off = L.gi_off + 16;
@@ -92,10 +106,10 @@ __device__ __forceinline__ ddc ddc_zero() { return ddc{dd_make(0.0), dd_make(0.0
 __device__ __forceinline__ ddc strip_pair_trace_dd(const double* X, const double* Y, int rows, int s,
                                                    int lane) {
   ddc acc = ddc_zero();
-  const int tot = rows * s;
+  const int tot = rows * s, prow = haf_dd_prow(s);
   for (int e = lane; e < tot; e += 32) {
     int i = e / s, t = e - i * s;
-    acc = ddc_add(acc, ddc_mul(ld_ddc(X + (i * s + t) * 4), ld_ddc(Y + ((i ^ 1) * s + (t ^ 1)) * 4)));
+    acc = ddc_add(acc, ddc_mul(ld_ddc(X + i * prow + t * 4), ld_ddc(Y + (i ^ 1) * prow + (t ^ 1) * 4)));
   }
   return warp_sum_ddc(acc);
 }
@@ -103,9 +117,10 @@ __device__ __forceinline__ ddc strip_pair_trace_dd(const double* X, const double
 __device__ __forceinline__ void strip_matvec_dd(const double* P, const double* Dv, double* Y, int col,
                                                 int hp1, int rows, int s, int lane) {
   const int i = lane >> 1, half = lane & 1;
+  const int prow = haf_dd_prow(s);
   ddc acc = ddc_zero();
   if (i < rows)
-    for (int t = half; t < s; t += 2) acc = ddc_add(acc, ddc_mul(ld_ddc(P + (i * s + t) * 4), ld_ddc(Dv + t * 4)));
+    for (int t = half; t < s; t += 2) acc = ddc_add(acc, ddc_mul(ld_ddc(P + i * prow + t * 4), ld_ddc(Dv + t * 4)));
   acc = ddc_add(acc, shfl_xor_ddc(acc, 1));
   if (half == 0 && i < 16) st_ddc(Y + (i * hp1 + col) * 4, i < rows ? acc : ddc_zero());
 }
@@ -199,9 +214,10 @@ static __device__ ddball haf_subset_term_dd(const double* __restrict__ A, int N,
     const int rows = min(16, s - r0);
     double* Pa = P0;
     double* Pb = P1;
+    const int prow = haf_dd_prow(s);
     for (int e = lane; e < 16 * s; e += 32) {
       int i = e / s;
-      st_ddc(Pa + e * 4, i < rows ? ld_ddc(Cs + ((r0 + i) * s + (e - i * s)) * 4) : ddc_zero());
+      st_ddc(Pa + i * prow + (e - i * s) * 4, i < rows ? ld_ddc(Cs + ((r0 + i) * s + (e - i * s)) * 4) : ddc_zero());
     }
     __syncwarp();
     {
@@ -221,8 +237,8 @@ static __device__ ddball haf_subset_term_dd(const double* __restrict__ A, int N,
         if (i < rows) {
           for (int j = j0; j < j1; ++j) {
             ddc acc = ddc_zero();
-            for (int t = 0; t < s; ++t) acc = ddc_add(acc, ddc_mul(ld_ddc(Pa + (i * s + t) * 4), ld_ddc(Cs + (t * s + j) * 4)));
-            st_ddc(Pb + (i * s + j) * 4, acc);
+            for (int t = 0; t < s; ++t) acc = ddc_add(acc, ddc_mul(ld_ddc(Pa + i * prow + t * 4), ld_ddc(Cs + (t * s + j) * 4)));
+            st_ddc(Pb + i * prow + j * 4, acc);
           }
         }
       }
