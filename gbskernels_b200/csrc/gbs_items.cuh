@@ -127,21 +127,15 @@ __device__ __noinline__ ItemResult haf_item(const double* __restrict__ mats, con
     // same grouping as the binary64 tiers (rings of kHafRing subsets, butterfly sum
     // per ring) so the certified value is the fp64 value bit for bit
     const HafLayout L = haf_layout(haf_smax, true);
-    double* ring = ws + L.ring_off;
+    double* ring = ws + L.cring_off;
     cball acc{mkc(0.0, 0.0), 0.0};
     int cnt = 0;
     for (unsigned long long k = 0; k < w.count; ++k) {
-      cball t = haf_subset_term_tc<true, REAL>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane);
-      if (lane == 0) {
-        ring[cnt * 3] = t.z.re;
-        ring[cnt * 3 + 1] = t.z.im;
-        ring[cnt * 3 + 2] = t.r;
-      }
+      // each subset parks its kg balls; kHafRing lanes then run the recurrences at once
+      haf_subset_term_tc<true, REAL>(A, N, n, (uint32_t)(w.lo + k), loop, ws, L, lane, ring + cnt * L.cslot);
       if (++cnt == kHafRing || k + 1 == w.count) {
         __syncwarp();
-        cball b{mkc(0.0, 0.0), 0.0};
-        if (lane < cnt) b = cball{mkc(ring[lane * 3], ring[lane * 3 + 1]), ring[lane * 3 + 2]};
-        acc = cb_add(acc, warp_sum_cb(b));
+        acc = cb_add(acc, haf_ring_flush_cert(ring, L.cslot, cnt, n, lane, ws + L.p_off));
         cnt = 0;
         __syncwarp();
       }

@@ -66,6 +66,9 @@ struct HafLayout {
   // certified tier only: |C|, the bound-path power, row bounds, trace-bound sums,
   // the Newton coefficients
   int ca_off, m_off, ym_off, bt_off, ev_off;
+  // certified tier: the ring of parked subsets' kg balls (cslot doubles per slot:
+  // entry 0 = sign, halving flag; entries 1..n = re, im, radius)
+  int cring_off, cslot;
 };
 __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   HafLayout L;
@@ -85,7 +88,7 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   L.ring_off = L.acc_off + 2 * np1 * 2;    // acc_p, acc_v
   L.total = L.ring_off + kHafRing * np1 * 2;
   L.total = (L.total + 1) & ~1;  // 16-byte multiple
-  L.ca_off = L.m_off = L.ym_off = L.bt_off = L.ev_off = 0;
+  L.ca_off = L.m_off = L.ym_off = L.bt_off = L.ev_off = L.cring_off = L.cslot = 0;
   if (cert) {
     L.ca_off = L.total;
     L.m_off = L.ca_off + rows * cs * 2;
@@ -94,6 +97,9 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
     L.ev_off = L.bt_off + 2 * (kHafMaxPairs + 2);
     L.total = L.ev_off + (kHafMaxPairs + 1) * 2;
     L.total = (L.total + 1) & ~1;
+    L.cslot = (3 * np1 + 1) & ~1;
+    L.cring_off = L.total;
+    L.total = L.cring_off + kHafRing * L.cslot;
   }
   return L;
 }
@@ -777,7 +783,6 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   int* gi = reinterpret_cast<int*>(ws + Lw.gi_off);
   double* acc_p = ws + Lw.acc_off;  // p[0..n]
   double* acc_v = acc_p + Lw.slot * 2;
-  double* ev = ws + Lw.ev_off;      // certified tier: the Newton coefficients
   double* Ca = ws + Lw.ca_off;
   double* M = ws + Lw.m_off;
   double* Ym = ws + Lw.ym_off;
@@ -906,7 +911,8 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
 
   // ---- Newton recurrence (certified: lane 0, then broadcast through shared memory;
   // binary64 tiers: kg_k parked by lane k, the recurrence runs in haf_ring_flush)
-  double* eb = bT;  // reused after the bounds are folded into kg (certified tier)
+  bool tiny_any = false;  // certified tier: a halving anywhere refuses the certificate
+  if constexpr (CERT) tiny_any = __any_sync(0xffffffffu, tiny_halving);
   if (!CERT || lane == 0) {
     if constexpr (CERT) {
       // value-path coefficients: E_a <= c_a M_a with M_a = |C|^a, M_a <= phi_a M^_a
@@ -959,15 +965,14 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
         }
         kgb[k] = g;
       }
-      cball e[kHafMaxPairs + 1];
-      e[0] = cball{mkc(1.0, 0.0), 0.0};
-      for (int j = 1; j <= n; ++j) {
-        cball acc{mkc(0.0, 0.0), 0.0};
-        for (int k = 1; k <= j; ++k) acc = cb_add(acc, cb_mul(kgb[k], e[j - k]));
-        e[j] = cb_div_int(acc, (double)j);
+      // parked for the recurrence (haf_ring_flush_cert: one lane per subset)
+      slot[0] = ((n - m) & 1) ? -1.0 : 1.0;
+      slot[1] = tiny_any ? 1.0 : 0.0;
+      for (int k = 1; k <= n; ++k) {
+        slot[3 * k] = kgb[k].z.re;
+        slot[3 * k + 1] = kgb[k].z.im;
+        slot[3 * k + 2] = kgb[k].r;
       }
-      st_c(ev + 2 * n, e[n].z);
-      eb[0] = e[n].r;
     } else {
       if (lane == 0) st_c(slot, mkc(((n - m) & 1) ? -1.0 : 1.0, 0.0));
       if (lane >= 1 && lane <= n) {
@@ -982,11 +987,46 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
   if constexpr (!CERT) {
     return cball{mkc(0.0, 0.0), 0.0};
   } else {
-    cplx coeff = ld_c(ev + 2 * n);
-    const double rad = __any_sync(0xffffffffu, tiny_halving) ? INFINITY : eb[0];
-    __syncwarp();
-    return cball{((n - m) & 1) ? cneg(coeff) : coeff, rad};
+    return cball{mkc(0.0, 0.0), 0.0};  // the term comes from haf_ring_flush_cert
   }
+}
+
+// Certified tier: the Newton recurrences of `cnt` parked subsets in ball arithmetic,
+// one lane each -- the operations of the one-subset recurrence, in its order, with
+// e_j interleaved in the idle power buffer `e` (3 doubles per ball) -- and the ball
+// sum of their signed terms over the lanes (warp_sum_cb, the grouping of the
+// binary64 ring, so the value is the fp64 value bit for bit).  A subset with a
+// halving that could round absolutely gets an infinite radius.
+__device__ __forceinline__ cball haf_ring_flush_cert(const double* ring, int slotw, int cnt, int n, int lane,
+                                                     double* e) {
+  cball b{mkc(0.0, 0.0), 0.0};
+  if (lane < cnt) {
+    const double* sl = ring + lane * slotw;
+    const double sign = sl[0];
+    if (sign != 0.0) {
+      double* el = e + lane * 3;
+      constexpr int es = kHafRing * 3;  // doubles between e_j and e_{j+1} of a lane
+      el[0] = 1.0;
+      el[1] = 0.0;
+      el[2] = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        cball acc{mkc(0.0, 0.0), 0.0};
+        for (int k = 1; k <= j; ++k) {
+          const double* ek = el + (j - k) * es;
+          acc = cb_add(acc, cb_mul(cball{mkc(sl[3 * k], sl[3 * k + 1]), sl[3 * k + 2]}, cball{mkc(ek[0], ek[1]), ek[2]}));
+        }
+        const cball ej = cb_div_int(acc, (double)j);
+        double* ed = el + j * es;
+        ed[0] = ej.z.re;
+        ed[1] = ej.z.im;
+        ed[2] = ej.r;
+      }
+      const double* en = el + n * es;
+      const cplx coeff = mkc(en[0], en[1]);
+      b = cball{sign < 0.0 ? cneg(coeff) : coeff, sl[1] != 0.0 ? INFINITY : en[2]};
+    }
+  }
+  return warp_sum_cb(b);
 }
 
 // Run the Newton recurrence of `cnt` parked subsets, one lane each, and return
