@@ -469,6 +469,15 @@ int sieve_run(const double* A_in, const double* gamma, int M, const int* reps, i
   if (e != cudaSuccess || dev < 0 || dev >= kSieveDevs)
     return sieve_fail(e != cudaSuccess ? (int)e : (int)cudaErrorInvalidDevice, "lhaf_repeated: no usable device");
   SieveBufs& Bf = g_sieve[dev];
+  if (Bf.coef) {
+    // a device reset (cudaDeviceReset) since the last call frees every allocation:
+    // the cached pointers then no longer name device memory, and are dropped
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, Bf.coef) != cudaSuccess || pa.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      Bf = SieveBufs{};
+    }
+  }
   if (!Bf.coef) {  // the tables, once per device
     e = cudaMalloc(&Bf.coef, sizeof(double) * T.coef.size());
     if (e == cudaSuccess) e = cudaMalloc(&Bf.bin, sizeof(double) * T.binom.size());
