@@ -121,8 +121,7 @@ extern "C" {
 //    gbs_set_split -- the same split gbs_haf_host uses, which keeps the values
 //    equal.  Larger requests return cudaErrorInvalidValue before any launch.
 //  * The first call on a device looks up the scratch array's device address
-//    (cudaGetSymbolAddress, with that device current); make that first call before
-//    any stream capture.
+//    (cudaGetSymbolAddress, with that device current) and keeps it.
 //  * Every call shares the one array and keeps the last call's contents (the fill
 //    kernel rewrites the queue and clears the counters each call); calls whose
 //    executions overlap on the GPU (different streams, or threads racing on one

@@ -275,8 +275,8 @@ int gbs_server_stats(gbs_server* sv, long long* completed, long long* batches, l
  * batch x 2^max(0, N/2 - 7) by default); larger requests return
  * cudaErrorInvalidValue.  The work queue is written on the device by a fill
  * kernel, so no host buffer is read after the call returns.  The first call on a
- * device looks up the array's address (make it before any stream capture); calls
- * that overlap on the GPU share the array and race.  Asynchronous on `stream` (a
+ * device looks up the array's address; calls that overlap on the GPU share the
+ * array and race.  Asynchronous on `stream` (a
  * cudaStream_t).  Values equal gbs_haf_host's bit for bit for complex input
  * (same split, same kernel).  Every input here runs the complex power loop: for a
  * real input (every imaginary part zero) gbs_haf_host runs the real one instead,
