@@ -83,7 +83,7 @@ __host__ __device__ inline HafLayout haf_layout(int smax, bool cert = false) {
   L.p_off = L.c_off + rows * cs * 2;       // C, every strip (zero padding rows)
   L.y_off = L.p_off + 16 * ps * 2;         // the power of one strip
   L.d_off = L.y_off + 16 * (h + 1) * 2;    // the loop vectors of one strip
-  L.gi_off = L.d_off + smax * 2;           // d
+  L.gi_off = L.d_off + ((smax + 3) & ~3) * 2;  // d, zero-padded to whole column tiles
   L.acc_off = L.gi_off + ((smax + 3) / 4) * 2;  // smax ints, 16-byte multiple
   L.ring_off = L.acc_off + 2 * np1 * 2;    // acc_p, acc_v
   L.total = L.ring_off + kHafRing * np1 * 2;
@@ -160,12 +160,11 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
     const double* bp1 = bptr + k1 * 4 * cs;
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-      if (nt < ntn) {
-        const double b0 = __longlong_as_double(__double_as_longlong(bp0[nt * 8]) ^ sgn);
-        const double b1 = __longlong_as_double(__double_as_longlong(bp1[nt * 8]) ^ sgn);
+      if (nt > 0 && nt >= ntn) break;  // the live tiles are a prefix: one exit test per tile
+      const double b0 = __longlong_as_double(__double_as_longlong(bp0[nt * 8]) ^ sgn);
+      const double b1 = __longlong_as_double(__double_as_longlong(bp1[nt * 8]) ^ sgn);
 #pragma unroll
-        for (int ms = 0; ms < MS; ++ms) dmma_m16n8k8(acc[k2][ms][nt], a0[ms], a1[ms], a2[ms], a3[ms], b0, b1);
-      }
+      for (int ms = 0; ms < MS; ++ms) dmma_m16n8k8(acc[k2][ms][nt], a0[ms], a1[ms], a2[ms], a3[ms], b0, b1);
     }
   };
   // a trailing single k4 slice when ksn is odd
@@ -179,11 +178,10 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
     const double* bp = bptr + ks * 4 * cs;
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-      if (nt < ntn) {
-        const double b = __longlong_as_double(__double_as_longlong(bp[nt * 8]) ^ sgn);
+      if (nt > 0 && nt >= ntn) break;
+      const double b = __longlong_as_double(__double_as_longlong(bp[nt * 8]) ^ sgn);
 #pragma unroll
-        for (int ms = 0; ms < MS; ++ms) dmma_m16n8k4(acc[k2][ms][nt], a0[ms], a1[ms], b);
-      }
+      for (int ms = 0; ms < MS; ++ms) dmma_m16n8k4(acc[k2][ms][nt], a0[ms], a1[ms], b);
     }
   };
   const int n8 = ksn >> 1;
@@ -249,73 +247,108 @@ __device__ __forceinline__ void store_acc(double* P, int ps, int s, int lane, co
     }
 }
 
-// Lane partial of sum_{i,t} D[i][t] * D[i^1][t^1] (partner in lane ^ 5, same slot).
-// (four independent accumulators: rows g / g + 8 x even / odd tiles)
-template <int NT, int MS>
-__device__ __forceinline__ cplx even_partial(const double (&D)[MS][NT][4], int ntn = NT) {
-  cplx acc[4] = {mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0)};
-#pragma unroll
-  for (int ms = 0; ms < MS; ++ms)
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      if (nt >= ntn) continue;  // tiles beyond the matrix are zero (warp-uniform)
-      const double p0 = shfl_xor_d(D[ms][nt][0], 5), p1 = shfl_xor_d(D[ms][nt][1], 5);
-      const double p2 = shfl_xor_d(D[ms][nt][2], 5), p3 = shfl_xor_d(D[ms][nt][3], 5);
-      acc[2 * (nt & 1)] = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), mkc(p0, p1), acc[2 * (nt & 1)]);
-      acc[2 * (nt & 1) + 1] = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), mkc(p2, p3), acc[2 * (nt & 1) + 1]);
-    }
-  return cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3]));
+// ---- one strip of a power in the binary64 value path.  The guards: LIVE (the 8-tile
+// path) keeps every live tile's four columns, including the columns s..4 ntn - 1,
+// which hold zeros wherever they are stored (the staged C, the powers, d); otherwise
+// (the 4-tile path, whose power stride can be below 4 ntn) only the columns < s.
+// The live tiles are a prefix, so a LIVE loop leaves at the first dead tile: one
+// warp-uniform exit test per tile instead of a divergent branch per column.
+template <int NT, bool LIVE>
+__device__ __forceinline__ bool strip_col(int nt, int ntn, int col, int s, bool& stop) {
+  stop = LIVE && nt > 0 && nt >= ntn;
+  return LIVE || col < s;
 }
 
-// Lane partial of sum_{i,t} D[i][t] * Q[i^1][t^1], Q the previous power in shared memory.
-template <int NT, int MS>
-__device__ __forceinline__ cplx odd_partial(const double (&D)[MS][NT][4], const double* Q, int ps, int s,
-                                            int lane) {
+// Load one strip (rows g / g + 8 of each tile, row stride ps complex) into the
+// accumulator layout; tiles not loaded hold zeros.
+template <int NT, bool LIVE>
+__device__ __forceinline__ void load_strip(const double* P, int ps, int s, int ntn, int lane, double (&D)[1][NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) D[0][nt][0] = D[0][nt][1] = D[0][nt][2] = D[0][nt][3] = 0.0;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const int col = 4 * nt + t4;
+    bool stop;
+    const bool use = strip_col<NT, LIVE>(nt, ntn, col, s, stop);
+    if (stop) break;
+    if (use) {
+      const cplx x0 = ld_c(P + (g * ps + col) * 2), x1 = ld_c(P + ((g + 8) * ps + col) * 2);
+      D[0][nt][0] = x0.re; D[0][nt][1] = x0.im; D[0][nt][2] = x1.re; D[0][nt][3] = x1.im;
+    }
+  }
+}
+
+template <int NT, bool LIVE>
+__device__ __forceinline__ void store_strip(double* P, int ps, int s, int ntn, int lane, const double (&D)[1][NT][4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const int col = 4 * nt + t4;
+    bool stop;
+    const bool use = strip_col<NT, LIVE>(nt, ntn, col, s, stop);
+    if (stop) break;
+    if (use) {
+      st_c(P + (g * ps + col) * 2, mkc(D[0][nt][0], D[0][nt][1]));
+      st_c(P + ((g + 8) * ps + col) * 2, mkc(D[0][nt][2], D[0][nt][3]));
+    }
+  }
+}
+
+// Lane partial of sum_{i,t} D[i][t] * Q[i^1][t^1] (four independent accumulators:
+// rows g / g + 8 x even / odd tiles).  Q = the previous power gives the odd trace
+// tr(C^{2a-1}); Q = D itself, once stored, the even trace tr(C^{2a}) (the partner
+// element is another lane's accumulator: reading it back from shared memory costs two
+// loads per tile where exchanging it costs eight shuffles).
+template <int NT, bool LIVE>
+__device__ __forceinline__ cplx pair_partial(const double (&D)[1][NT][4], const double* Q, int ps, int s, int ntn,
+                                             int lane) {
   const int g = lane >> 2, t4 = lane & 3;
   cplx acc[4] = {mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0), mkc(0.0, 0.0)};
 #pragma unroll
-  for (int ms = 0; ms < MS; ++ms)
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      const int col = 4 * nt + t4;
-      if (col < s) {
-        const int cp = col ^ 1;
-        const cplx q0 = ld_c(Q + ((16 * ms + (g ^ 1)) * ps + cp) * 2);
-        const cplx q1 = ld_c(Q + ((16 * ms + ((g + 8) ^ 1)) * ps + cp) * 2);
-        acc[2 * (nt & 1)] = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), q0, acc[2 * (nt & 1)]);
-        acc[2 * (nt & 1) + 1] = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), q1, acc[2 * (nt & 1) + 1]);
-      }
+  for (int nt = 0; nt < NT; ++nt) {
+    const int col = 4 * nt + t4;
+    bool stop;
+    const bool use = strip_col<NT, LIVE>(nt, ntn, col, s, stop);
+    if (stop) break;
+    if (use) {
+      const int cp = col ^ 1;
+      const cplx q0 = ld_c(Q + ((g ^ 1) * ps + cp) * 2);
+      const cplx q1 = ld_c(Q + (((g + 8) ^ 1) * ps + cp) * 2);
+      acc[2 * (nt & 1)] = cfma(mkc(D[0][nt][0], D[0][nt][1]), q0, acc[2 * (nt & 1)]);
+      acc[2 * (nt & 1) + 1] = cfma(mkc(D[0][nt][2], D[0][nt][3]), q1, acc[2 * (nt & 1) + 1]);
     }
+  }
   return cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3]));
 }
 
 // y[row] = sum_t D[row][t] d[t] for the rows of this lane's group; lanes t4 == 0
 // write Y[row * hp1 + col].
-template <int NT, int MS>
-__device__ __forceinline__ void rows_times_d(const double (&D)[MS][NT][4], const double* Dv, double* Y, int col,
-                                             int hp1, int s, int lane) {
+template <int NT, bool LIVE>
+__device__ __forceinline__ void rows_times_d(const double (&D)[1][NT][4], const double* Dv, double* Y, int col,
+                                             int hp1, int s, int ntn, int lane) {
   const int g = lane >> 2, t4 = lane & 3;
+  cplx y0 = mkc(0.0, 0.0), y1 = mkc(0.0, 0.0);
 #pragma unroll
-  for (int ms = 0; ms < MS; ++ms) {
-    cplx y0 = mkc(0.0, 0.0), y1 = mkc(0.0, 0.0);
+  for (int nt = 0; nt < NT; ++nt) {
+    const int c = 4 * nt + t4;
+    bool stop;
+    const bool use = strip_col<NT, LIVE>(nt, ntn, c, s, stop);
+    if (stop) break;
+    if (use) {
+      const cplx dv = ld_c(Dv + c * 2);
+      y0 = cfma(mkc(D[0][nt][0], D[0][nt][1]), dv, y0);
+      y1 = cfma(mkc(D[0][nt][2], D[0][nt][3]), dv, y1);
+    }
+  }
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      const int c = 4 * nt + t4;
-      if (c < s) {
-        const cplx dv = ld_c(Dv + c * 2);
-        y0 = cfma(mkc(D[ms][nt][0], D[ms][nt][1]), dv, y0);
-        y1 = cfma(mkc(D[ms][nt][2], D[ms][nt][3]), dv, y1);
-      }
-    }
-#pragma unroll
-    for (int m = 1; m <= 2; m <<= 1) {
-      y0.re += shfl_xor_d(y0.re, m); y0.im += shfl_xor_d(y0.im, m);
-      y1.re += shfl_xor_d(y1.re, m); y1.im += shfl_xor_d(y1.im, m);
-    }
-    if (t4 == 0) {
-      st_c(Y + ((16 * ms + g) * hp1 + col) * 2, y0);
-      st_c(Y + ((16 * ms + g + 8) * hp1 + col) * 2, y1);
-    }
+  for (int m = 1; m <= 2; m <<= 1) {
+    y0.re += shfl_xor_d(y0.re, m); y0.im += shfl_xor_d(y0.im, m);
+    y1.re += shfl_xor_d(y1.re, m); y1.im += shfl_xor_d(y1.im, m);
+  }
+  if (t4 == 0) {
+    st_c(Y + (g * hp1 + col) * 2, y0);
+    st_c(Y + ((g + 8) * hp1 + col) * 2, y1);
   }
 }
 
@@ -426,35 +459,36 @@ __device__ __noinline__ void haf_powers(const double* Cs, double* P, double* Y, 
   const int strips = haf_strips(s);
   const int vq = (lane >> 3) & 3;          // the total this lane holds after warp_sum4_scatter
   const bool vlead = (lane & 7) == 0;
+  constexpr bool LIVE = NT == 8;  // the 8-tile power stride holds every live tile's columns
   for (int ms = 0; ms < strips; ++ms) {
     const int r0 = 16 * ms;
     const double* Cstrip = Cs + r0 * cs * 2;
     double D[1][NT][4];
     if (loop && lane < 16) st_c(Y + (lane * hp1) * 2, r0 + lane < s ? ld_c(Dv + (r0 + lane) * 2) : mkc(0.0, 0.0));
     // power 1 (= the strip of C, read in place with stride cs): p_2 and y_1
-    load_acc<NT, 1>(Cstrip, cs, s, lane, D);
+    load_strip<NT, LIVE>(Cstrip, cs, s, ntn, lane, D);
     {
-      const cplx t = even_partial<NT, 1>(D, ntn);
+      const cplx t = pair_partial<NT, LIVE>(D, Cstrip, cs, s, ntn, lane);
       const double tot = warp_sum4_scatter(t.re, t.im, 0.0, 0.0, lane);
       if (vlead && vq < 2 && 2 <= n) acc_p[4 + vq] += tot;
     }
-    if (loop) rows_times_d<NT, 1>(D, Dv, Y, 1, hp1, s, lane);
+    if (loop) rows_times_d<NT, LIVE>(D, Dv, Y, 1, hp1, s, ntn, lane);
     for (int a = 2; a <= h; ++a) {
       // the previous power: the strip of C (stride cs) for a = 2, then P (stride ps), in place
       const double* Q = (a == 2) ? Cstrip : P;
       const int qs = (a == 2) ? cs : ps;
       power_product<NT, 1>(Q, Cs, s, cs, qs, ntn, lane, D);
-      const cplx to = odd_partial<NT, 1>(D, Q, qs, s, lane);
-      const cplx te = even_partial<NT, 1>(D, ntn);
+      const cplx to = pair_partial<NT, LIVE>(D, Q, qs, s, ntn, lane);  // odd trace, before Q is overwritten
+      __syncwarp();
+      store_strip<NT, LIVE>(P, ps, s, ntn, lane, D);
+      if (loop) rows_times_d<NT, LIVE>(D, Dv, Y, a, hp1, s, ntn, lane);
+      __syncwarp();
+      const cplx te = pair_partial<NT, LIVE>(D, P, ps, s, ntn, lane);  // even trace, from the stored power
       const double tot = warp_sum4_scatter(to.re, to.im, te.re, te.im, lane);
       if (vlead) {
         const int k = vq < 2 ? 2 * a - 1 : 2 * a;
         if (k <= n) acc_p[2 * k + (vq & 1)] += tot;
       }
-      __syncwarp();
-      store_acc<NT, 1>(P, ps, s, lane, D);
-      if (loop) rows_times_d<NT, 1>(D, Dv, Y, a, hp1, s, lane);
-      __syncwarp();
     }
     if (loop) {
       // this strip's share of v_k (lane k - 1, rows in order)
@@ -804,6 +838,22 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
     // rows s..rows-1 stay zero: they are the padding rows of the power-2 A operand
     const int dr = 32 / ccols, dc = 32 - dr * ccols;  // (r, c) advance per 32 elements
     int r = lane / ccols, c = lane - (lane / ccols) * ccols;
+    if constexpr (!CERT) {
+      // without divergent branches: rows < s element by element (a padding column
+      // loads a valid entry and stores zero), then the padding rows as zeros over the
+      // whole row stride.  The symmetric part (A + A^T)/2 is staged: see below.
+      for (int e = lane; e < s * ccols; e += 32, r += dr, c += dc) {
+        const bool wrap = c >= ccols;
+        c = wrap ? c - ccols : c;
+        r = wrap ? r + 1 : r;
+        const bool in = c < s;
+        const int rr = gi[r], cc = gi[in ? (c ^ 1) : 0];  // X swaps the columns within each pair
+        const cplx x = ld_c(A + ((size_t)rr * N + cc) * 2), y = ld_c(A + ((size_t)cc * N + rr) * 2);
+        const cplx v = cscale(cadd(x, y), 0.5);
+        st_c(Cs + (r * cs + c) * 2, (in && (loop || rr != cc)) ? v : mkc(0.0, 0.0));
+      }
+      for (int e = lane; e < (rows - s) * cs; e += 32) st_c(Cs + (s * cs + e) * 2, mkc(0.0, 0.0));
+    } else
     for (int e = lane; e < rows * ccols; e += 32, r += dr, c += dc) {
       if (c >= ccols) {
         c -= ccols;
@@ -833,6 +883,7 @@ static __device__ cball haf_subset_term_tc(const double* __restrict__ A, int N, 
       if constexpr (CERT) st_c(Ca + (r * cs + c) * 2, mkc(ru_abs_c(v), 0.0));
     }
     if (loop && lane < s) st_c(Dv + lane * 2, ld_c(A + ((size_t)gi[lane] * N + gi[lane]) * 2));
+    else if (loop && lane < ((s + 3) & ~3)) st_c(Dv + lane * 2, mkc(0.0, 0.0));  // whole column tiles
   }
   for (int k = lane; k <= n; k += 32) {
     st_c(acc_p + 2 * k, mkc(0.0, 0.0));
