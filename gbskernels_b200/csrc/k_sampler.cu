@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -255,23 +256,38 @@ int sampler_fail(int code, const std::string& msg) {
   return code;
 }
 
-struct SamplerBufs {
-  double *Ak = nullptr, *invfac = nullptr, *sub = nullptr, *part = nullptr, *paux = nullptr, *out = nullptr,
-         *aux = nullptr;
-  int *state = nullptr, *head = nullptr, *done = nullptr, *pst = nullptr, *st = nullptr, *overflow = nullptr;
-  InstDesc* insts = nullptr;
-  WorkItem* items = nullptr;
-  // prefix deduplication: the table (keys, representative draw, slot number), each
-  // draw's slot, the unique prefixes' representatives and their count
-  unsigned long long* tkeys = nullptr;
-  int *trep = nullptr, *sid = nullptr, *slot_of = nullptr, *urep = nullptr, *nuniq = nullptr;
-  ~SamplerBufs() {
-    for (void* p : {(void*)Ak, (void*)invfac, (void*)sub, (void*)part, (void*)paux, (void*)out, (void*)aux,
-                    (void*)state, (void*)head, (void*)done, (void*)pst, (void*)st, (void*)overflow, (void*)insts,
-                    (void*)items, (void*)tkeys, (void*)trep, (void*)sid, (void*)slot_of, (void*)urep, (void*)nuniq})
-      if (p) cudaFree(p);
+// Device buffers of the chain, kept per device between calls and grown only when a
+// call needs more: allocating and freeing them per call (cudaFree synchronises the
+// device) cost more host time than the chain's kernels on 100,000 draws, and made
+// the call time vary several-fold from run to run.  Calls hold g_sampler_mu.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  cudaError_t need(size_t n) {
+    n = std::max<size_t>(n, 1);
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const cudaError_t e = cudaMalloc(&p, sizeof(T) * n);
+    if (e == cudaSuccess) cap = n;
+    return e;
   }
 };
+struct SamplerBufs {
+  DevBuf<double> Ak, invfac, sub, part, paux, out, aux;
+  DevBuf<int> state, head, done, pst, st, overflow;
+  DevBuf<InstDesc> insts;
+  DevBuf<WorkItem> items;
+  // prefix deduplication: the table (keys, representative draw, slot number), each
+  // draw's slot, the unique prefixes' representatives and their count
+  DevBuf<unsigned long long> tkeys;
+  DevBuf<int> trep, sid, slot_of, urep, nuniq;
+};
+constexpr int kSamplerDevs = 64;
+SamplerBufs g_sampler[kSamplerDevs];
+std::mutex g_sampler_mu;
 
 // The chain over modes 1..M for draws [0, num_draws), in chunks whose conditional
 // submatrices fit the slot budget.  weights_out (optional, testing): the Re(haf)
@@ -294,7 +310,20 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
   for (int k = 1; k <= M; ++k)
     if (h_off[k - 1] < 0 || (long long)h_off[k - 1] + 4ll * k * k > ak_total)
       return sampler_fail((int)cudaErrorInvalidValue, "sampler: A_k offsets outside the buffer");
-  SamplerBufs B;
+  std::lock_guard<std::mutex> lk(g_sampler_mu);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSamplerDevs)
+    return sampler_fail((int)cudaErrorInvalidDevice, "sampler: no usable device");
+  SamplerBufs& B = g_sampler[dev];
+  if (B.overflow.p) {
+    // a device reset (cudaDeviceReset) since the last call frees every allocation:
+    // the cached pointers then no longer name device memory, and are dropped
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, B.overflow.p) != cudaSuccess || pa.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      B = SamplerBufs{};
+    }
+  }
   const int per = cutoff + 1;
   const int slot_max = std::max(2, std::min(kSamplerMaxN, 2 * M * cutoff));
   // work items per instance at most (2^7 subsets each)
@@ -324,62 +353,61 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
   const int ninst = ucap * per;
   const size_t nitem_cap = (size_t)ninst * max_split;
   if (nitem_cap > (size_t)INT32_MAX) return sampler_fail((int)cudaErrorInvalidValue, "sampler: too many work items");
-  cudaError_t e = cudaMalloc(&B.Ak, sizeof(double) * 2 * std::max<long long>(ak_total, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&B.invfac, sizeof(double) * per);
-  if (e == cudaSuccess) e = cudaMalloc(&B.sub, (size_t)ninst * slot_max * slot_max * 16);
-  if (e == cudaSuccess) e = cudaMalloc(&B.part, sizeof(double) * 4 * nitem_cap);
-  if (e == cudaSuccess) e = cudaMalloc(&B.paux, sizeof(double) * nitem_cap);
-  if (e == cudaSuccess) e = cudaMalloc(&B.out, sizeof(double) * 2 * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.aux, sizeof(double) * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.state, sizeof(int) * (size_t)num_draws * M);
-  if (e == cudaSuccess) e = cudaMalloc(&B.head, sizeof(int) * 2);  // queue head, item count
-  if (e == cudaSuccess) e = cudaMalloc(&B.done, sizeof(int) * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.pst, sizeof(int) * nitem_cap);
-  if (e == cudaSuccess) e = cudaMalloc(&B.st, sizeof(int) * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.overflow, sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&B.insts, sizeof(InstDesc) * ninst);
-  if (e == cudaSuccess) e = cudaMalloc(&B.items, sizeof(WorkItem) * nitem_cap);
+  cudaError_t e = B.Ak.need(2 * (size_t)std::max<long long>(ak_total, 1));
+  if (e == cudaSuccess) e = B.invfac.need(per);
+  if (e == cudaSuccess) e = B.sub.need((size_t)ninst * slot_max * slot_max * 2);
+  if (e == cudaSuccess) e = B.part.need(4 * nitem_cap);
+  if (e == cudaSuccess) e = B.paux.need(nitem_cap);
+  if (e == cudaSuccess) e = B.out.need(2 * (size_t)ninst);
+  if (e == cudaSuccess) e = B.aux.need(ninst);
+  if (e == cudaSuccess) e = B.state.need((size_t)num_draws * M);
+  if (e == cudaSuccess) e = B.head.need(2);  // queue head, item count
+  if (e == cudaSuccess) e = B.done.need(ninst);
+  if (e == cudaSuccess) e = B.pst.need(nitem_cap);
+  if (e == cudaSuccess) e = B.st.need(ninst);
+  if (e == cudaSuccess) e = B.overflow.need(1);
+  if (e == cudaSuccess) e = B.insts.need(ninst);
+  if (e == cudaSuccess) e = B.items.need(nitem_cap);
   int tsize = 1;
   while (tsize < 2 * chunk) tsize <<= 1;
-  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.tkeys, sizeof(unsigned long long) * tsize);
-  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.trep, sizeof(int) * tsize);
-  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.sid, sizeof(int) * tsize);
-  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.slot_of, sizeof(int) * chunk);
-  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.urep, sizeof(int) * chunk);
-  if (dedup && e == cudaSuccess) e = cudaMalloc(&B.nuniq, sizeof(int));
+  if (dedup && e == cudaSuccess) e = B.tkeys.need(tsize);
+  if (dedup && e == cudaSuccess) e = B.trep.need(tsize);
+  if (dedup && e == cudaSuccess) e = B.sid.need(tsize);
+  if (dedup && e == cudaSuccess) e = B.slot_of.need(chunk);
+  if (dedup && e == cudaSuccess) e = B.urep.need(chunk);
+  if (dedup && e == cudaSuccess) e = B.nuniq.need(1);
   if (e != cudaSuccess) return sampler_fail((int)e, "sampler: device allocation failed");
   cudaStream_t s = nullptr;
   e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e != cudaSuccess) return sampler_fail((int)e, "sampler: stream");
-  e = cudaMemcpyAsync(B.Ak, h_Ak, sizeof(double) * 2 * ak_total, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(B.invfac, h_invfac, sizeof(double) * per, cudaMemcpyHostToDevice, s);
+  e = cudaMemcpyAsync(B.Ak.p, h_Ak, sizeof(double) * 2 * ak_total, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(B.invfac.p, h_invfac, sizeof(double) * per, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     if (h_state_in)
-      e = cudaMemcpyAsync(B.state, h_state_in, sizeof(int) * (size_t)num_draws * M, cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync(B.state.p, h_state_in, sizeof(int) * (size_t)num_draws * M, cudaMemcpyHostToDevice, s);
     else
-      e = cudaMemsetAsync(B.state, 0, sizeof(int) * (size_t)num_draws * M, s);
+      e = cudaMemsetAsync(B.state.p, 0, sizeof(int) * (size_t)num_draws * M, s);
   }
-  if (e == cudaSuccess) e = cudaMemsetAsync(B.overflow, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B.overflow.p, 0, sizeof(int), s);
   // the hafnian launch: one-warp blocks, the grid from the occupancy of the kernel
   constexpr unsigned BR = br1(kFnHaf, kTierFp64);
   ItemLaunch L{};
-  L.mats = B.sub;
-  L.insts = B.insts;
-  L.items = B.items;
+  L.mats = B.sub.p;
+  L.insts = B.insts.p;
+  L.items = B.items.p;
   L.order = nullptr;
-  L.head = B.head;
-  L.done = B.done;
-  L.part = B.part;
-  L.paux = B.paux;
-  L.pst = B.pst;
-  L.out = B.out;
-  L.aux_out = B.aux;
-  L.st_out = B.st;
-  L.n_items_dev = B.head + 1;
+  L.head = B.head.p;
+  L.done = B.done.p;
+  L.part = B.part.p;
+  L.paux = B.paux.p;
+  L.pst = B.pst.p;
+  L.out = B.out.p;
+  L.aux_out = B.aux.p;
+  L.st_out = B.st.p;
+  L.n_items_dev = B.head.p + 1;
   L.haf_smax = slot_max;
   L.ws_doubles = (haf_layout(slot_max).total + 3) & ~3;
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
+  int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int bps = occ_br<BR>(L, 1);
   if (bps <= 0) {
@@ -395,29 +423,29 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
     for (int k = kfirst; k <= kmax && e == cudaSuccess; ++k) {
       const int slot = std::max(2, std::min(kSamplerMaxN, 2 * k * cutoff));
       if (dedup) {
-        e = cudaMemsetAsync(B.tkeys, 0xFF, sizeof(unsigned long long) * tsize, s);
+        e = cudaMemsetAsync(B.tkeys.p, 0xFF, sizeof(unsigned long long) * tsize, s);
         if (e == cudaSuccess) {
-          sampler_key_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.state, M, d0, nd, k, per, B.tkeys, B.trep, tsize - 1,
-                                                              B.slot_of);
+          sampler_key_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.state.p, M, d0, nd, k, per, B.tkeys.p, B.trep.p, tsize - 1,
+                                                              B.slot_of.p);
           e = cudaGetLastError();
         }
         if (e == cudaSuccess) {
-          sampler_compact_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.tkeys, B.trep, tsize, B.sid, B.urep, B.nuniq);
+          sampler_compact_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.tkeys.p, B.trep.p, tsize, B.sid.p, B.urep.p, B.nuniq.p);
           e = cudaGetLastError();
         }
         if (e != cudaSuccess) break;
       }
-      sampler_gather_kernel<<<(ni + 127) / 128, 128, 0, s>>>(B.Ak + 2 * (size_t)h_off[k - 1], k, B.state, M, d0, nd,
-                                                            cutoff, slot, B.sub, B.insts, B.overflow,
-                                                            dedup ? B.urep : nullptr, dedup ? B.nuniq : nullptr);
+      sampler_gather_kernel<<<(ni + 127) / 128, 128, 0, s>>>(B.Ak.p + 2 * (size_t)h_off[k - 1], k, B.state.p, M, d0, nd,
+                                                            cutoff, slot, B.sub.p, B.insts.p, B.overflow.p,
+                                                            dedup ? B.urep.p : nullptr, dedup ? B.nuniq.p : nullptr);
       e = cudaGetLastError();
       if (e == cudaSuccess) {
-        sampler_plan_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.insts, ni, B.items, B.head + 1,
-                                                             dedup ? B.nuniq : nullptr, per);
+        sampler_plan_kernel<<<1, kSamplerPlanThreads, 0, s>>>(B.insts.p, ni, B.items.p, B.head.p + 1,
+                                                             dedup ? B.nuniq.p : nullptr, per);
         e = cudaGetLastError();
       }
-      if (e == cudaSuccess) e = cudaMemsetAsync(B.head, 0, sizeof(int), s);
-      if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, sizeof(int) * std::min(ni, ninst), s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(B.head.p, 0, sizeof(int), s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(B.done.p, 0, sizeof(int) * std::min(ni, ninst), s);
       if (e == cudaSuccess) {
         L.n_items = (int)nitem_cap;  // upper bound; the kernel reads the planned count
         e = launch_br<BR>(L, sms * bps, 1, s);
@@ -425,20 +453,20 @@ int sampler_chain(const double* h_Ak, long long ak_total, const int* h_off, int 
       if (e != cudaSuccess) break;
       if (weights_out && k == kmax) {
         std::vector<double> o(2 * (size_t)ni);
-        e = cudaMemcpyAsync(o.data(), B.out, sizeof(double) * 2 * ni, cudaMemcpyDeviceToHost, s);
+        e = cudaMemcpyAsync(o.data(), B.out.p, sizeof(double) * 2 * ni, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         for (int t = 0; t < ni && e == cudaSuccess; ++t) weights_out[(size_t)d0 * per + t] = o[2 * (size_t)t];
         break;
       }
-      sampler_draw_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.out, B.invfac, cutoff, d0, nd, seed, k, B.state, M,
-                                                           dedup ? B.slot_of : nullptr, dedup ? B.sid : nullptr);
+      sampler_draw_kernel<<<(nd + 127) / 128, 128, 0, s>>>(B.out.p, B.invfac.p, cutoff, d0, nd, seed, k, B.state.p, M,
+                                                           dedup ? B.slot_of.p : nullptr, dedup ? B.sid.p : nullptr);
       e = cudaGetLastError();
     }
   }
   int over = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&over, B.overflow, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&over, B.overflow.p, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && h_out)
-    e = cudaMemcpyAsync(h_out, B.state, sizeof(int) * (size_t)num_draws * M, cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(h_out, B.state.p, sizeof(int) * (size_t)num_draws * M, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cudaStreamDestroy(s);
   if (e != cudaSuccess) return sampler_fail((int)e, std::string("sampler: ") + cudaGetErrorString(e));
