@@ -538,10 +538,10 @@ def main():
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
                          # DRAM read + write bytes of one launch: an ncu capture of this
-                         # kernel on the 256-instance case (--profile-small) read 2.066944 MB
+                         # kernel on the 256-instance case (--profile-small) read 1.741568 MB
                          # and wrote 0 B; scaled by the instances per launch (each matrix is
                          # read once, so DRAM traffic grows in proportion)
-                         "traffic": 2.066944e6 / 256 * B,
+                         "traffic": 1.741568e6 / 256 * B,
                          "traffic_unit": "bytes per launch (ncu capture scaled by instances)",
                          "peak_source": "FP64 mma.m16n8k8 throughput measured live (gbs_probe_fp64_peak); "
                                         "MEASURED_PEAKS.json has no FP64 figure",
