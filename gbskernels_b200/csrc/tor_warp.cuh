@@ -50,6 +50,8 @@
 // of every pivot and the final rsqrt (tor_cert_rho).
 #pragma once
 
+#include <type_traits>
+
 #include "cert.cuh"
 #include "gbs_common.cuh"
 
@@ -153,7 +155,11 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
   // forward substitution over the existing columns v < R0 (owners of v < 32 hold the
   // residual in slot 0, the others in slot 1)
   double* cv = col;  // column v starts at tor_col_base(v, rows)
-  auto step = [&](int v, double av, double bv) {
+  // NS residual slots per lane take part: when every slot fits one warp (nx <= 32,
+  // warp-uniform) the second slot is idle throughout and its update is skipped
+  // (it would be fma(-0, l, 0) == 0: the values do not change)
+  auto step = [&](auto ns, int v, double av, double bv) {
+    constexpr int NS = decltype(ns)::value;
     const double iv = inv[v];
     const double l0 = av * iv, l1 = bv * iv;
     if (lane == (v & 31)) {
@@ -161,7 +167,7 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
       cv[R1 - v] = l1;
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NS; ++h) {
       double e = 0.0;  // 0 for finished or idle slots: fma(-0, l, a) == a
       if (v < lim[h]) e = cv[off[h] - v];
       a[h] = fma(-e, l0, a[h]);
@@ -173,10 +179,16 @@ __device__ __forceinline__ bool tor_w_append(const double* __restrict__ Oc, int 
     cv += rows + kTorTD - v;
   };
   const int v1 = R0 < 32 ? R0 : 32;
-  for (int v = 0; v < v1; ++v)
-    step(v, __shfl_sync(0xffffffffu, a[0], v), __shfl_sync(0xffffffffu, b[0], v));
-  for (int v = 32; v < R0; ++v)
-    step(v, __shfl_sync(0xffffffffu, a[1], v & 31), __shfl_sync(0xffffffffu, b[1], v & 31));
+  if (nx <= 32) {
+    for (int v = 0; v < v1; ++v)
+      step(std::integral_constant<int, 1>{}, v, __shfl_sync(0xffffffffu, a[0], v), __shfl_sync(0xffffffffu, b[0], v));
+  } else {
+    for (int v = 0; v < v1; ++v)
+      step(std::integral_constant<int, 2>{}, v, __shfl_sync(0xffffffffu, a[0], v), __shfl_sync(0xffffffffu, b[0], v));
+    for (int v = 32; v < R0; ++v)
+      step(std::integral_constant<int, 2>{}, v, __shfl_sync(0xffffffffu, a[1], v & 31),
+           __shfl_sync(0xffffffffu, b[1], v & 31));
+  }
   // the two pivots (identical in every lane)
   double s0 = d00;
   bool ok = s0 > 0.0;
