@@ -100,7 +100,8 @@ int gbs_tor_single_ddcertified_host(const double* O, int n, int g, double* out, 
  * ordinary hafnian of the expansion); reps: batch x M non-negative counts; out:
  * batch complex values lhaf(A repeated by reps[b]).  Caps: M <= 32, N = sum(reps[b])
  * <= 64, prod(reps[b][i] + 1) <= 2^40.  A non-symmetric A enters as its symmetric
- * part (A + A^T)/2, the only part x^T A x sees.                                    */
+ * part (A + A^T)/2, the only part x^T A x sees.  The sieve's device buffers stay
+ * allocated on each device between calls (grown only); calls are serialised.      */
 int gbs_lhaf_repeated_host(const double* A, const double* gamma, int M, const int* reps, int batch, double* out);
 /* certified sieve: values bit-identical to gbs_lhaf_repeated_host and a rigorous
  * bound per pattern (bound[b] >= |out[b] - lhaf|); non-finite input is rejected, an
@@ -122,7 +123,9 @@ const char* gbs_lhaf_repeated_last_error(void);
  * uniform per draw and mode, subsequence = draw index); h_out: num_draws x M counts.
  * Draws that share a prefix (the counts of the modes before k) share their
  * conditional hafnians, which are evaluated once per distinct prefix.
- * Requires 2 M cutoff <= 32 (maxn is accepted for the reference's signature).      */
+ * Requires 2 M cutoff <= 32 (maxn is accepted for the reference's signature).  The
+ * chain's device buffers stay allocated on each device between calls (grown only);
+ * calls are serialised.                                                            */
 int gbs_sampler_sample(const double* h_Ak, int ak_total, const int* h_off, int M, int num_draws, int cutoff,
                        int maxn, const double* h_invfac, unsigned long long seed, int* h_out);
 /* the conditional weights Re haf(A_k[idx, idx]) of mode k for the prefixes in
