@@ -24,8 +24,11 @@
 //     so powers up to h = ceil(n/2) give every trace p_1..p_n: h-1 products per
 //     subset instead of the reference's n-1.  In the mma accumulator layout the
 //     partner element (i^1, t^1) of a lane's element sits in lane ^ 5, same
-//     register: the even trace is a shuffle, the odd one reads the previous power,
-//     which is then overwritten in place.
+//     register; both traces read it from shared memory: the odd one from the
+//     previous power before it is overwritten in place, the even one from the new
+//     power once stored.
+//   * The live column tiles of a subset are a prefix, so every tile loop leaves at
+//     the first dead tile (one warp-uniform test per tile).
 //   * Loop term: with y_a = C^a d, d^T X C^{a+b} d = (X y_a)^T y_b, so
 //     v_k = (1/2) sum_i y_a[i^1] y_b[i] with a + b = k - 1 from the same powers.
 #pragma once
