@@ -161,13 +161,21 @@ __device__ __forceinline__ void power_product(const double* __restrict__ P, cons
     }
     const double* bp0 = bptr + k0 * 4 * cs;
     const double* bp1 = bptr + k1 * 4 * cs;
+    // the live tiles are a prefix: one exit test per tile; the next live tile's
+    // fragments are loaded before this tile's mma, so their latency overlaps it
+    double nb0 = bp0[0], nb1 = bp1[0];
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-      if (nt > 0 && nt >= ntn) break;  // the live tiles are a prefix: one exit test per tile
-      const double b0 = __longlong_as_double(__double_as_longlong(bp0[nt * 8]) ^ sgn);
-      const double b1 = __longlong_as_double(__double_as_longlong(bp1[nt * 8]) ^ sgn);
+      const double b0 = __longlong_as_double(__double_as_longlong(nb0) ^ sgn);
+      const double b1 = __longlong_as_double(__double_as_longlong(nb1) ^ sgn);
+      const bool more = nt + 1 < NT && nt + 1 < ntn;
+      if (more) {
+        nb0 = bp0[(nt + 1) * 8];
+        nb1 = bp1[(nt + 1) * 8];
+      }
 #pragma unroll
       for (int ms = 0; ms < MS; ++ms) dmma_m16n8k8(acc[k2][ms][nt], a0[ms], a1[ms], a2[ms], a3[ms], b0, b1);
+      if (!more) break;
     }
   };
   // a trailing single k4 slice when ksn is odd
